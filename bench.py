@@ -1,0 +1,393 @@
+"""Benchmark of the neural wavelet PRT relight pass (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision auto|bf16|fp32] [--workload relight1080|sh1080]
+
+Default workload: relight of a 1920x1080 synthetic G-buffer with K=300 wavelets of a
+6x64x64 env map through the 16-level hash grid + 64-wide MLP network (FP16-rounded
+random-init params).  One step = TCNNPass_p1 + TCNNPass_p2 of one frame.  Metric:
+pixel*wavelet evaluations per second, whole job.
+
+Multi-GPU (torchrun): every rank relights its own frame (request-level data
+parallelism, no collective on the data path); timing is the max over ranks.
+
+``--impl reference`` times the reference's relighting math on the host cores (the CPU
+oracle, all threads) on a bounded pixel sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "px*wavelet evals/s at 1080p K=300"
+WIDTH, HEIGHT, K_WAVELETS = 1920, 1080, 300
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["auto", "bf16", "fp32"], default="auto")
+    ap.add_argument("--workload", choices=["relight1080", "sh1080"], default="relight1080")
+    ap.add_argument("--fp32-steps", type=int, default=2, help="timed steps of the plain FP32 path")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------- helpers
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def load_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------- workload
+
+def make_relight_inputs(rank: int):
+    from neural_wavelet_prt_demo_b200 import netconfig, synth
+    desc = netconfig.parse(netconfig.CONFIG_LARGE)
+    w = synth.make_weights(desc, seed=0, hash_scale=1e-4, param_round="fp16")
+    gb = synth.make_gbuffer(WIDTH, HEIGHT, seed=1 + rank)
+    faces = synth.make_env_faces(desc.face_size, seed=2)
+    return desc, w, gb, faces
+
+
+def cpu_relight_rate(desc, w, gb, idx, st, budget_s: float):
+    """Oracle FP32 relight on a contiguous block of pixels sized to ~budget_s of host time."""
+    from oracle import oracle as O
+    b = O.Bound(desc, w, gb)
+    threads = O.max_threads()
+    mid = gb.n // 2
+    n = 256
+    t0 = time.perf_counter()
+    O.relight_f32(b, idx, st, px_begin=mid, px_end=mid + n, n_threads=threads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(gb.n - mid, max(n, n * budget_s / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    O.relight_f32(b, idx, st, px_begin=mid, px_end=mid + n2, n_threads=threads)
+    dt = time.perf_counter() - t0
+    return n2 * len(idx) / dt, threads, n2, dt
+
+
+# ---------------------------------------------------------------------------- ours
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from neural_wavelet_prt_demo_b200 import engine as eng
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+
+    if args.workload == "sh1080":
+        return run_sh(args, rank, world, local, dev)
+
+    desc, w, gb, faces = make_relight_inputs(rank)
+    e = eng.RenderEngine(netconfig_json(), device=local)
+    e.loadWeights(w)
+    env_id = e.addEnvironmentMap(eng.EnvironmentMap(faces), K=K_WAVELETS)
+    idx, st = e.envWavelets(env_id)
+    fr = eng.FullFrame.from_gbuffer(gb, dev)
+    e.setFrame(0, fr)
+    N = WIDTH * HEIGHT
+    evals = N * K_WAVELETS
+
+    precision = args.precision
+    if precision == "auto":
+        try:
+            e.TCNNPass_p1(0)
+            e.TCNNPass_p2(env_id, 0, eng.RenderConfig(precision="bf16"))
+            e.TCNNSync()
+            precision = "bf16"
+        except eng.NwprtError:
+            precision = "fp32"
+    cfg = eng.RenderConfig(precision=precision)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        e.TCNNPass_p1(0)
+        e.TCNNPass_p2(env_id, 0, cfg)
+
+    def timed(step_fn, steps, warmup, kernel_events=None):
+        for _ in range(warmup):
+            step_fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            step_fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps
+
+    # ---- device-resident throughput (value) with live per-launch kernel timing
+    kev = []
+
+    def step_k():
+        e.TCNNPass_p1(0)
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        e.TCNNPass_p2(env_id, 0, cfg)
+        s1.record(stream)
+        kev.append((s0, s1))
+
+    sampler = ClockSampler(local)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler.start()
+    ms_step = timed(step_k, args.steps, 0)
+    clocks = sampler.stop()
+    kernel_ms = sum(x.elapsed_time(y) for x, y in kev) / len(kev)
+    value = world * evals / (ms_step / 1e3)
+
+    # ---- end to end through the public API with host buffers
+    pin = lambda t: t.cpu().pin_memory()
+    host_in = {n: pin(getattr(fr, n)) for n in ("fbFirstHitPos", "fbworldNormal", "fbFirstHitReflecDir",
+                                                 "fbRoughness", "fbFirstHitKd", "fbFirstHitKs",
+                                                 "fbDirectDenoised", "fbEnvironmentMapFlag")}
+    host_out = {n: torch.empty_like(getattr(fr, n), device="cpu").pin_memory()
+                for n in ("fbPredictedIndirect", "fbPredictedIndirectWithDirect")}
+    h2d = sum(t.numel() * t.element_size() for t in host_in.values())
+    d2h = sum(t.numel() * t.element_size() for t in host_out.values())
+
+    def step_e2e():
+        for n, t in host_in.items():
+            getattr(fr, n).copy_(t, non_blocking=True)
+        step()
+        for n, t in host_out.items():
+            t.copy_(getattr(fr, n), non_blocking=True)
+
+    ms_e2e = timed(step_e2e, max(3, args.steps // 2), 1)
+    e2e = {"value": world * evals / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
+
+    # ---- the plain FP32 drop-in path, same workload (for the served/plain ratio)
+    plain = None
+    if precision != "fp32" and args.fp32_steps > 0:
+        cfg32 = eng.RenderConfig(precision="fp32")
+
+        def step32():
+            e.TCNNPass_p1(0)
+            e.TCNNPass_p2(env_id, 0, cfg32)
+
+        ms32 = timed(step32, args.fp32_steps, 1)
+        plain = {"value": world * evals / (ms32 / 1e3), "unit": "evals/s", "ms_per_step": ms32}
+
+    # ---- roofline of the dominant kernel (the fused relight)
+    peaks, peak_src = load_peaks()
+    flops = desc.flops_per_eval() * evals
+    achieved = flops / (kernel_ms / 1e3) / 1e12
+    if precision == "bf16":
+        peak = peaks.get("bf16_tflops_sustained") or peaks["bf16_tflops"]
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": f"{peak_src} bf16 sustained (kernel runs back to back for the whole step)"}
+    else:
+        peak = 148 * 128 * 2 * 1.965e9 / 1e12
+        roof = {"bound": "fp32-simt", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 FMA/clk x 1965 MHz)"}
+    roof["kernel_ms"] = kernel_ms
+    roof["algorithmic_flops_per_launch"] = flops
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, n_px, dt = cpu_relight_rate(desc, w, gb, idx, st, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "evals/s", "cores": cores, "kind": "port",
+               "sample": f"{n_px} contiguous pixels x K={K_WAVELETS} through the FP32 oracle ({dt:.1f} s)"}
+
+    e.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": precision,
+            "data": "synthetic: seeded G-buffer, log-normal env map, random-init FP16-rounded weights",
+            "config": {"workload": "relight 1920x1080, K=300 of a 6x64x64 env map, hash 16x2 2^19, "
+                                   "MLPs 32->64x3->64 | 80->64x3->3",
+                       "pixels_per_gpu": N, "K": K_WAVELETS, "precision": precision,
+                       "l2": "inputs 209 MB/frame > 126 MB L2 (no flush)",
+                       "parallelism": f"request-dp{world}", "step": "TCNNPass_p1 + TCNNPass_p2"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
+            "clocks": clocks, "plain_fp32": plain,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def netconfig_json():
+    from neural_wavelet_prt_demo_b200 import netconfig
+    return netconfig.to_json(netconfig.CONFIG_LARGE)
+
+
+# ---------------------------------------------------------------------------- SH workload
+
+def run_sh(args, rank, world, local, dev):
+    import torch
+    import torch.distributed as dist
+    from neural_wavelet_prt_demo_b200 import engine as eng, synth
+    N = WIDTH * HEIGHT
+    g = torch.Generator(device=dev).manual_seed(rank)
+    l = torch.floor(torch.sqrt(torch.arange(81, device=dev, dtype=torch.float32))).clamp_min(1)
+    T = torch.randn((N, 81), generator=g, device=dev) / (l * l)
+    faces = torch.from_numpy(synth.make_env_faces(128, seed=0)).to(dev)
+    L = eng.sh_project(faces)
+    out = torch.empty((N, 4), device=dev)
+    for _ in range(args.warmup):
+        eng.sh_dot(T, L, out=out)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        eng.sh_dot(T, L, out=out)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    bytes_ = N * 81 * 4 + N * 16 + 81 * 12
+    peaks, src = load_peaks()
+    gbs = bytes_ / (ms / 1e3) / 1e9
+    if rank == 0:
+        print(json.dumps({"metric": "SH dot GB/s at 1080p (81 coeffs)", "value": gbs * world, "unit": "GB/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic", "config": {"workload": "sh_dot 1920x1080x81"},
+                          "roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                       "frac": gbs / peaks["hbm_gbs"], "traffic": None},
+                          "gpu_launches": args.steps}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from neural_wavelet_prt_demo_b200 import netconfig
+    desc, w, gb, faces = make_relight_inputs(0)
+    idx, st = O.haar_topk(faces, K_WAVELETS)
+    per_step = max(1.0, 150.0 / (args.steps + args.warmup))
+    rate0, cores, n_px, _ = cpu_relight_rate(desc, w, gb, idx, st, per_step)
+    b = O.Bound(desc, w, gb)
+    mid = gb.n // 2
+    for _ in range(args.warmup):
+        O.relight_f32(b, idx, st, px_begin=mid, px_end=mid + n_px, n_threads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.relight_f32(b, idx, st, px_begin=mid, px_end=mid + n_px, n_threads=cores)
+    dt = (time.perf_counter() - t0) / args.steps
+    rate = n_px * K_WAVELETS / dt
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "relight 1920x1080, K=300 (host-core sample)", "K": K_WAVELETS,
+                       "pixels_per_step": n_px},
+            "cpu_baseline": {"value": rate, "unit": "evals/s", "cores": cores, "kind": "port",
+                             "sample": f"{n_px} pixels x K={K_WAVELETS} per step, FP32 oracle "
+                                       "(the reference's relight math restated; tiny-cuda-nn absent)"},
+            "e2e": {"value": rate, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

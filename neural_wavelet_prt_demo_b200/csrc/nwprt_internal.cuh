@@ -1,0 +1,231 @@
+// Internal declarations shared by the libnwprt translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nwprt.h"
+
+namespace nwprt {
+
+// ------------------------------------------------------------------ errors
+struct Error : std::runtime_error {
+  nwprt_status status;
+  Error(nwprt_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(nwprt_status s, const std::string& m) { throw Error(s, m); }
+
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation)
+      fail(NWPRT_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+    fail(NWPRT_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+#define NWPRT_CUDA(call) ::nwprt::cuda_check((call), #call)
+
+// Device-side error codes (written to a device error word, read by the host).
+enum DevError : uint32_t {
+  kDevOk = 0,
+  kDevWaitTimeout = 1,  // a bounded mbarrier wait ran out
+  kDevBadIndex = 2,     // a gather index outside its table (input validation)
+};
+
+// ------------------------------------------------------------------ network
+constexpr int kMaxLevels = 32;
+constexpr int kMaxLayers = 8;
+
+struct NetDims {
+  int n_levels = 0, n_features = 0, log2_table = 0, base_resolution = 0;
+  double per_level_scale = 0;
+  int level_res[kMaxLevels] = {0};
+  int level_size[kMaxLevels] = {0};
+  int level_offset[kMaxLevels] = {0};
+  int aux_width = 16;
+  int op_neurons = 64, op_hidden = 0, op_out = 64;
+  int cn_neurons = 64, cn_hidden = 0;
+  int face_size = 64;
+  int op_nl = 0, op_in[kMaxLayers] = {0}, op_outs[kMaxLayers] = {0};
+  int cn_nl = 0, cn_in[kMaxLayers] = {0}, cn_outs[kMaxLayers] = {0};
+
+  int enc_dims() const { return n_levels * n_features; }
+  int n_coeffs() const { return 6 * face_size * face_size; }
+  size_t n_hash_params() const {
+    size_t s = 0;
+    for (int l = 0; l < n_levels; ++l) s += (size_t)level_size[l];
+    return s * (size_t)n_features;
+  }
+  size_t n_op_params() const {
+    size_t s = 0;
+    for (int i = 0; i < op_nl; ++i) s += (size_t)op_in[i] * op_outs[i];
+    return s;
+  }
+  size_t n_cn_params() const {
+    size_t s = 0;
+    for (int i = 0; i < cn_nl; ++i) s += (size_t)cn_in[i] * cn_outs[i];
+    return s;
+  }
+  double flops_per_eval() const;
+};
+
+NetDims parse_config(const std::string& json_text);
+
+// Hash-grid level table passed by value to kernels.
+struct HashLevels {
+  int n_levels, n_features;
+  int res[kMaxLevels];
+  uint32_t size[kMaxLevels];
+  uint32_t offset[kMaxLevels];
+  uint32_t dense_mask;  // bit l set: level l indexes its table densely
+};
+
+// ------------------------------------------------------------------ npy / json helpers
+struct NpyArray {
+  std::vector<size_t> shape;
+  std::string descr;
+  std::vector<char> data;
+};
+NpyArray read_npy(const std::string& path);
+
+// ------------------------------------------------------------------ kernels (launchers)
+// haar_topk.cu
+void launch_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx, float* strength,
+                      uint32_t* err, cudaStream_t st);
+size_t haar_topk_smem_bytes(int S, int K);
+
+// sh.cu
+size_t sh_project_workspace_bytes(int S);
+void launch_sh_project(const float* faces, int S, float* L, float* workspace, cudaStream_t st);
+void launch_sh_dot(const float* T, int64_t n_px, int nc, const float* L, int abs_out, float* out,
+                   uint32_t* err, cudaStream_t st);
+
+// relight_common.cu
+void launch_pack_gbuffer(const nwprt_gbuffer& g, float* packed, cudaStream_t st);
+void launch_gather_embedding(const float* emb, int D, int n_coeffs, const int32_t* idx, int K,
+                             float* out_kd, uint32_t* err, cudaStream_t st);
+
+// One relight job: a prepared frame and an env wavelet table.
+struct RelightJob {
+  const float* packed;    // [n_px][16]
+  const uint8_t* flag;    // [n_px]
+  const float* direct;    // float4 [n_px]
+  const float* emb_k;     // [K][D] embedding gathered at the env's indices (FP32)
+  const float* strength;  // [K][3]
+  int K;
+  int64_t n_px;
+  float* indirect;
+  float* with_direct;
+};
+
+struct DeviceWeights {
+  const float* hash;       // [sum T_l][F]
+  const float* op_t;       // out_prd layers transposed [in][out_pad4], FP32
+  const float* cn_t;       // cmp_net layers transposed
+  size_t op_t_floats, cn_t_floats;
+};
+
+// relight_fp32.cu
+bool relight_fp32_supported(const NetDims& d, std::string* why);
+void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWeights& w,
+                         const RelightJob& job, int clamp, int kahan, cudaStream_t st);
+// Host-side packing of FP32 weights into the kernel's transposed layout.
+void pack_fp32_weights(const NetDims& d, const float* op, const float* cn,
+                       std::vector<float>* op_t, std::vector<float>* cn_t);
+
+// relight_tc.cu (tcgen05 BF16 path)
+bool relight_tc_supported(const NetDims& d, std::string* why);
+size_t tc_weight_bytes(const NetDims& d);
+void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);
+size_t tc_env_table_bytes(const NetDims& d, int K);
+void launch_tc_env_table(const NetDims& d, const uint16_t* tc_weights_dev, const float* emb_k,
+                         int K, uint16_t* table, cudaStream_t st);
+struct TcJob {
+  const float* packed;
+  const uint8_t* flag;
+  const float* direct;
+  const uint16_t* env_table;  // per-k first-layer weights, pre-swizzled BF16
+  const float* strength;
+  int K;
+  int64_t n_px;
+  float* indirect;
+  float* with_direct;
+};
+void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash,
+                       const uint16_t* tc_weights_dev, const TcJob* jobs, int n_jobs,
+                       TcJob* jobs_dev, int kahan, int clamp, uint32_t* err, cudaStream_t st);
+
+}  // namespace nwprt
+
+// ------------------------------------------------------------------ device helpers
+#ifdef __CUDACC__
+namespace nwprt {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Bounded mbarrier wait.  Returns false (and records kDevWaitTimeout) when the
+// phase did not complete within `limit` polls; callers then abandon their work.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err,
+                                          uint32_t limit = (1u << 26)) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  if (err) atomicCAS(err, 0u, (uint32_t)kDevWaitTimeout);
+  return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completion on `bar` (no multicast).
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace nwprt
+#endif

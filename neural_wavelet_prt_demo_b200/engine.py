@@ -1,0 +1,346 @@
+"""Python host mirror of the reference's neural-relight interface over libnwprt.
+
+Names and argument meaning follow the reference so callers and tests read alike:
+
+* ``RenderEngine``   -- ``initTCNN`` / ``TCNNAvaliable`` / ``TCNNPass_p1`` /
+  ``TCNNPass_p2`` / ``TCNNSync`` / ``buildLights`` (Renderer/RenderEngine.h:58-83,
+  Renderer/tinycudann/tcnn.cu:49-162).
+* ``EnvironmentMap`` -- ``faces``, ``topWaveletCoefficients``, ``topWaveletStrength``,
+  ``shCoefficients`` (Renderer/EnvironmentMap.h:11-40).
+* ``FullFrame``      -- the fullFrameCUDA fields the relight reads and writes
+  (Renderer/frames.h:96-214).
+* ``RenderConfig``   -- renderConfig (Renderer/RenderEngine.h:29-42) plus the relight
+  arithmetic options.
+
+Errors raise (``NwprtError``), as the reference's CUDA_CHECK throws
+std::runtime_error (Renderer/optix7.h:27-38).  torch only provides device memory and
+streams; every computation runs in libnwprt.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import NwprtError, check, lib
+from . import netconfig
+
+__all__ = ["RenderEngine", "EnvironmentMap", "FullFrame", "RenderConfig", "NwprtError",
+           "haar_topk", "sh_project", "sh_dot"]
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream_ptr(stream) -> C.c_void_p:
+    if stream is None:
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, torch.cuda.Stream):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+@dataclass
+class RenderConfig:
+    """renderConfig (RenderEngine.h:29-42) fields that matter to the relight, plus
+    the arithmetic of the transport MLP."""
+    waveletMode: bool = True
+    precision: str = "fp32"        # "fp32" (drop-in) | "bf16" (tcgen05)
+    clamp_terms: bool = True       # utils_kernels.h:87-89 max(L*T, 0)
+    kahan: bool = True
+
+    def opts(self) -> _lib.RelightOpts:
+        prec = {"fp32": _lib.PREC_FP32, "bf16": _lib.PREC_BF16}.get(self.precision)
+        if prec is None:
+            raise ValueError(f"unknown precision {self.precision!r}")
+        return _lib.RelightOpts(prec, int(self.clamp_terms), int(self.kahan))
+
+
+@dataclass
+class FullFrame:
+    """Device G-buffer + relight outputs of one frame (frames.h:143-183 field names)."""
+    width: int
+    height: int
+    fbFirstHitPos: torch.Tensor
+    fbworldNormal: torch.Tensor
+    fbFirstHitReflecDir: torch.Tensor
+    fbRoughness: torch.Tensor
+    fbFirstHitKd: torch.Tensor
+    fbFirstHitKs: torch.Tensor
+    fbDirectDenoised: torch.Tensor
+    fbEnvironmentMapFlag: torch.Tensor
+    fbPredictedIndirect: torch.Tensor
+    fbPredictedIndirectWithDirect: torch.Tensor
+
+    @staticmethod
+    def from_gbuffer(gb, device="cuda:0") -> "FullFrame":
+        """From a synth.GBuffer (numpy) -> device tensors, outputs zero-initialised."""
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+        n = gb.width * gb.height
+        return FullFrame(gb.width, gb.height, t(gb.pos), t(gb.normal), t(gb.reflect), t(gb.roughness),
+                         t(gb.kd), t(gb.ks), t(gb.direct), t(gb.flag),
+                         torch.zeros((n, 4), dtype=torch.float32, device=device),
+                         torch.zeros((n, 4), dtype=torch.float32, device=device))
+
+    def gbuffer_struct(self) -> _lib.GBuffer:
+        for name in ("fbFirstHitPos", "fbworldNormal", "fbFirstHitReflecDir", "fbFirstHitKd",
+                     "fbFirstHitKs", "fbDirectDenoised"):
+            t = getattr(self, name)
+            if t.dtype != torch.float32 or not t.is_contiguous() or t.numel() != 4 * self.width * self.height:
+                raise ValueError(f"{name} must be a contiguous float32 [N,4] tensor")
+        if self.fbRoughness.dtype != torch.float32 or self.fbRoughness.numel() != self.width * self.height:
+            raise ValueError("fbRoughness must be float32 [N]")
+        if self.fbEnvironmentMapFlag.dtype not in (torch.uint8, torch.bool):
+            raise ValueError("fbEnvironmentMapFlag must be uint8 or bool")
+        return _lib.GBuffer(self.width, self.height, *[
+            _ptr(getattr(self, n)) for n in ("fbFirstHitPos", "fbworldNormal", "fbFirstHitReflecDir",
+                                             "fbRoughness", "fbFirstHitKd", "fbFirstHitKs",
+                                             "fbDirectDenoised", "fbEnvironmentMapFlag")])
+
+
+class EnvironmentMap:
+    """Environment_Map (EnvironmentMap.h:11-40): cubemap faces and their wavelet table.
+
+    ``faces`` is float32 [6, S, S, 3] in the reference face order (+X,-X,+Y,-Y,-Z,+Z).
+    The wavelet table either comes from precomputed arrays (the reference's
+    waveletcoeffs/ + waveletstrength/ npy pair) or is computed on the GPU by
+    ``computeWavelets`` (Haar + top-K).
+    """
+
+    def __init__(self, faces: Optional[np.ndarray] = None, top_coefficients=None, top_strength=None,
+                 sh_coefficients=None):
+        self.faces = None if faces is None else np.ascontiguousarray(faces, np.float32)
+        self.topWaveletCoefficients = (None if top_coefficients is None
+                                       else np.ascontiguousarray(top_coefficients, np.int32).ravel())
+        self.topWaveletStrength = (None if top_strength is None
+                                   else np.ascontiguousarray(top_strength, np.float32).reshape(-1, 3))
+        self.shCoefficients = None if sh_coefficients is None else np.asarray(sh_coefficients, np.float32)
+
+    @staticmethod
+    def cross_to_faces(cross: np.ndarray, from_npy: bool = True) -> np.ndarray:
+        """4x3 cross image [3S, 4S, 3] -> faces (EnvironmentMap.cpp:80-126).
+        ``.npy`` crosses are flipped vertically first, as loadCubeMap does (:96-101)."""
+        img = np.asarray(cross, np.float32)
+        if from_npy:
+            img = img[::-1]
+        S = img.shape[0] // 3
+        if img.shape[1] != 4 * S:
+            raise ValueError("cross image must be 3S x 4S")
+        # get_submatrix(from_c, from_r, ...) offsets in face units, initCubeFaces order
+        cells = [(2, 1), (0, 1), (1, 2), (1, 0), (1, 1), (3, 1)]
+        return np.stack([img[r * S:(r + 1) * S, c * S:(c + 1) * S] for c, r in cells]).copy()
+
+    @staticmethod
+    def from_folder(folder: str, name: str) -> "EnvironmentMap":
+        """Environment_Map(envMapFolder, envMapName) for .npy assets: cube/<name>.npy,
+        waveletcoeffs/<name>.npy, waveletstrength/<name>.npy, sh/<name>.npy (EnvironmentMap.cpp:20-68)."""
+        if not os.path.isdir(folder):
+            raise RuntimeError("Invalid Env map Folder Name, it should not be a file")
+        cube = os.path.join(folder, "cube", name + ".npy")
+        if not os.path.exists(cube):
+            raise RuntimeError("Invalid Env map File Name")
+        faces = EnvironmentMap.cross_to_faces(np.load(cube), from_npy=True)
+        em = EnvironmentMap(faces)
+        wc = os.path.join(folder, "waveletcoeffs", name + ".npy")
+        ws = os.path.join(folder, "waveletstrength", name + ".npy")
+        if os.path.exists(wc) and os.path.exists(ws):
+            st = np.load(ws)
+            if st.ndim != 2 or st.shape[1] != 3:
+                raise RuntimeError("waveletstrength must be [K, 3]")
+            em.topWaveletCoefficients = np.ascontiguousarray(np.load(wc), np.int32).ravel()
+            em.topWaveletStrength = np.ascontiguousarray(st, np.float32)
+        sh = os.path.join(folder, "sh", name + ".npy")
+        if os.path.exists(sh):
+            em.shCoefficients = np.load(sh).astype(np.float32)
+        return em
+
+    def computeWavelets(self, K: int, device="cuda:0") -> None:
+        """Haar transform + top-K selection on the GPU; fills the two wavelet arrays."""
+        f = torch.from_numpy(self.faces).to(device)
+        idx, st = haar_topk(f, K)
+        self.topWaveletCoefficients = idx.cpu().numpy()
+        self.topWaveletStrength = st.cpu().numpy()
+
+    def computeSH(self, device="cuda:0") -> None:
+        f = torch.from_numpy(self.faces).to(device)
+        self.shCoefficients = sh_project(f).cpu().numpy()
+
+
+class RenderEngine:
+    """The reference RenderEngine's neural-relight surface over one libnwprt context."""
+
+    def __init__(self, config, device: int = 0, debug: bool = False):
+        if isinstance(config, dict):
+            config = json.dumps(config)
+        self.desc = netconfig.parse(config)
+        self.device = device
+        self.debug = debug
+        self._ctx = C.c_void_p()
+        check(lib().nwprt_create(config.encode(), device, C.byref(self._ctx)))
+        self.fullframeCUDABuffer: List[Optional[FullFrame]] = [None, None]
+        self.envIds: List[int] = []
+        self.TCNNSetup = False
+        self.EnvmapSetup = False
+
+    # ---------------------------------------------------------------- lifetime
+    def close(self):
+        if self._ctx:
+            lib().nwprt_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status):
+        check(status, self._ctx)
+
+    # ---------------------------------------------------------------- weights
+    def initTCNN(self, modelPath: str) -> None:
+        """RenderEngine::initTCNN(modelPath): loads vtx_enc/out_prd/cmp_net/wve_enc .npy."""
+        self._check(lib().nwprt_load_weights_dir(self._ctx, modelPath.encode()))
+        self.TCNNSetup = True
+
+    def loadWeights(self, w) -> None:
+        """Same from in-memory arrays (a synth.Weights)."""
+        arrs = [np.ascontiguousarray(a, np.float32).ravel()
+                for a in (w.hash_params, w.out_prd, w.cmp_net, w.wve_enc)]
+        ws = _lib.Weights(arrs[0].ctypes.data, arrs[0].size, arrs[1].ctypes.data, arrs[1].size,
+                          arrs[2].ctypes.data, arrs[2].size, arrs[3].ctypes.data, arrs[3].size)
+        self._check(lib().nwprt_load_weights(self._ctx, C.byref(ws)))
+        self.TCNNSetup = True
+
+    def TCNNAvaliable(self) -> bool:
+        return bool(lib().nwprt_ready(self._ctx))
+
+    def networkInfo(self) -> _lib.NetworkInfo:
+        info = _lib.NetworkInfo()
+        self._check(lib().nwprt_get_network_info(self._ctx, C.byref(info)))
+        return info
+
+    # ---------------------------------------------------------------- env maps
+    def addEnvironmentMap(self, env: EnvironmentMap, K: Optional[int] = None, stream=None) -> int:
+        """Registers one env map; returns its envMapID.  With K given (or no precomputed
+        table) the wavelet table is computed on the GPU from the faces."""
+        env_id = C.c_int(-1)
+        if K is not None or env.topWaveletCoefficients is None:
+            if env.faces is None:
+                raise ValueError("env map has neither faces nor a wavelet table")
+            K = 64 if K is None else K
+            self._check(lib().nwprt_env_from_faces(
+                self._ctx, env.faces.ctypes.data_as(C.c_void_p), 0, env.faces.shape[1], int(K),
+                _stream_ptr(stream), C.byref(env_id)))
+        else:
+            idx = np.ascontiguousarray(env.topWaveletCoefficients, np.int32)
+            st = np.ascontiguousarray(env.topWaveletStrength, np.float32)
+            if st.shape != (idx.size, 3):
+                raise ValueError("topWaveletStrength must be [K, 3] matching the coefficients")
+            self._check(lib().nwprt_env_from_wavelets(
+                self._ctx, idx.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p), idx.size, 0,
+                _stream_ptr(stream), C.byref(env_id)))
+        self.envIds.append(env_id.value)
+        self.EnvmapSetup = True
+        return len(self.envIds) - 1
+
+    def buildLights(self, envMaps: List[EnvironmentMap], K: Optional[int] = None) -> None:
+        """RenderEngine::buildLights (RenderEngine.cpp:113-175): registers every env map."""
+        for e in envMaps:
+            self.addEnvironmentMap(e, K)
+
+    def envWavelets(self, envMapID: int):
+        env_id = self.envIds[envMapID]
+        K = C.c_int(0)
+        self._check(lib().nwprt_env_get_wavelets(self._ctx, env_id, None, None, 0, C.byref(K)))
+        idx = np.empty(K.value, np.int32)
+        st = np.empty((K.value, 3), np.float32)
+        self._check(lib().nwprt_env_get_wavelets(self._ctx, env_id, idx.ctypes.data_as(C.c_void_p),
+                                                 st.ctypes.data_as(C.c_void_p), K.value, C.byref(K)))
+        return idx, st
+
+    # ---------------------------------------------------------------- frames
+    def setFrame(self, frameID: int, frame: FullFrame) -> None:
+        while len(self.fullframeCUDABuffer) <= frameID:
+            self.fullframeCUDABuffer.append(None)
+        self.fullframeCUDABuffer[frameID] = frame
+
+    def TCNNPass_p1(self, frameID: int, stream=None) -> None:
+        """tcnn.cu:83-108: the frame's G-buffer -> packed per-pixel input rows."""
+        f = self.fullframeCUDABuffer[frameID]
+        if f is None:
+            raise RuntimeError(f"frame {frameID} has no buffers (setFrame first)")
+        gb = f.gbuffer_struct()
+        self._check(lib().nwprt_prepare(self._ctx, frameID, C.byref(gb), _stream_ptr(stream)))
+
+    def TCNNPass_p2(self, envMapID: int, frameID: int, config: Optional[RenderConfig] = None,
+                    stream=None) -> None:
+        """tcnn.cu:111-152: relight the prepared frame with env `envMapID` into the frame's
+        fbPredictedIndirect / fbPredictedIndirectWithDirect.  Asynchronous."""
+        config = config or RenderConfig()
+        f = self.fullframeCUDABuffer[frameID]
+        opts = config.opts()
+        self._check(lib().nwprt_relight(self._ctx, self.envIds[envMapID], frameID, C.byref(opts),
+                                        _ptr(f.fbPredictedIndirect), _ptr(f.fbPredictedIndirectWithDirect),
+                                        _stream_ptr(stream)))
+
+    def relightBatch(self, requests, config: Optional[RenderConfig] = None, stream=None) -> None:
+        """Several (envMapID, frameID, indirect, with_direct) relights in one device pass."""
+        config = config or RenderConfig()
+        arr = (_lib.Request * len(requests))()
+        for i, (e, fr, ind, wd) in enumerate(requests):
+            arr[i] = _lib.Request(self.envIds[e], fr, ind.data_ptr(), wd.data_ptr())
+        opts = config.opts()
+        self._check(lib().nwprt_relight_batch(self._ctx, arr, len(requests), C.byref(opts),
+                                              _stream_ptr(stream)))
+
+    def TCNNSync(self) -> None:
+        """tcnn.cu:154-158; also surfaces device-side error reports."""
+        self._check(lib().nwprt_sync(self._ctx))
+
+
+# -------------------------------------------------------------------- context-free kernels
+
+def haar_topk(faces: torch.Tensor, K: int, stream=None):
+    """faces float32 cuda [6,S,S,3] or [E,6,S,S,3] -> (idx int32 [..,K], strength [..,K,3])."""
+    if faces.dtype != torch.float32 or not faces.is_cuda or not faces.is_contiguous():
+        raise ValueError("faces must be a contiguous float32 CUDA tensor")
+    batched = faces.dim() == 5
+    f = faces if batched else faces.unsqueeze(0)
+    E, S = f.shape[0], f.shape[2]
+    idx = torch.empty((E, K), dtype=torch.int32, device=faces.device)
+    st = torch.empty((E, K, 3), dtype=torch.float32, device=faces.device)
+    check(lib().nwprt_haar_topk(_ptr(f), E, S, int(K), _ptr(idx), _ptr(st), _stream_ptr(stream)))
+    return (idx, st) if batched else (idx[0], st[0])
+
+
+def sh_project(faces: torch.Tensor, stream=None) -> torch.Tensor:
+    """faces float32 cuda [6,S,S,3] -> L [81,3] (order-8 SH of the cubemap)."""
+    if faces.dtype != torch.float32 or not faces.is_cuda or not faces.is_contiguous():
+        raise ValueError("faces must be a contiguous float32 CUDA tensor")
+    S = faces.shape[1]
+    nbytes = lib().nwprt_sh_project_workspace_size(S)
+    ws = torch.empty(max(1, nbytes // 4), dtype=torch.float32, device=faces.device)
+    L = torch.empty((81, 3), dtype=torch.float32, device=faces.device)
+    check(lib().nwprt_sh_project(_ptr(faces), S, _ptr(L), _ptr(ws), nbytes, _stream_ptr(stream)))
+    return L
+
+
+def sh_dot(T: torch.Tensor, L: torch.Tensor, abs_out: bool = True, out: Optional[torch.Tensor] = None,
+           stream=None) -> torch.Tensor:
+    """T float32 cuda [N, nc], L [nc, 3] -> out [N, 4] = (|T L|, 1)."""
+    if T.dtype != torch.float32 or not T.is_contiguous() or L.dtype != torch.float32:
+        raise ValueError("T and L must be contiguous float32")
+    N, nc = T.shape
+    if out is None:
+        out = torch.empty((N, 4), dtype=torch.float32, device=T.device)
+    check(lib().nwprt_sh_dot(_ptr(T), N, nc, _ptr(L.contiguous()), int(abs_out), _ptr(out),
+                             _stream_ptr(stream)))
+    return out

@@ -1,0 +1,46 @@
+"""Shared case builders and error metrics for the test suite."""
+from dataclasses import dataclass
+
+import numpy as np
+
+from neural_wavelet_prt_demo_b200 import netconfig, synth
+from oracle import oracle as O
+
+
+@dataclass
+class Case:
+    desc: object
+    cfg: dict
+    weights: object
+    gbuf: object
+    faces: np.ndarray
+    idx: np.ndarray
+    strength: np.ndarray
+    bound: object
+
+
+def make_case(cfg, width, height, K, seed=0, hash_scale=1e-4, flag_prob=1.0, param_round="fp32"):
+    desc = netconfig.parse(cfg)
+    w = synth.make_weights(desc, seed=seed, hash_scale=hash_scale, param_round=param_round)
+    gb = synth.make_gbuffer(width, height, seed=seed + 1, flag_prob=flag_prob)
+    faces = synth.make_env_faces(desc.face_size, seed=seed + 2)
+    idx, st = O.haar_topk(faces, K)
+    return Case(desc, cfg, w, gb, faces, idx, st, O.Bound(desc, w, gb))
+
+
+def rel_err(x, ref, floor_frac=1e-6):
+    x = np.asarray(x, np.float64)
+    ref = np.asarray(ref, np.float64)
+    floor = max(floor_frac * float(np.abs(ref).max()), 1e-30)
+    e = np.abs(x - ref) / np.maximum(np.abs(ref), floor)
+    return float(e.max()), float(e.mean())
+
+
+def psnr(x, ref):
+    x = np.asarray(x, np.float64)
+    ref = np.asarray(ref, np.float64)
+    mse = float(np.mean((x - ref) ** 2))
+    peak = float(np.abs(ref).max())
+    if mse == 0:
+        return float("inf")
+    return 10.0 * np.log10(peak * peak / mse)

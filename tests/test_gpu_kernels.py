@@ -1,0 +1,95 @@
+"""GPU parity of the env-map kernels through the C ABI: Haar + top-K (bit-exact),
+SH projection (FP32 vs the FP64 oracle) and the SH dot product (bit-exact vs the FP32 oracle)."""
+import numpy as np
+import pytest
+
+from neural_wavelet_prt_demo_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine():
+    from neural_wavelet_prt_demo_b200 import engine
+    return engine
+
+
+@pytest.mark.parametrize("S,K", [(1, 1), (1, 6), (2, 5), (4, 96), (8, 64), (8, 384), (16, 300), (32, 64),
+                                 (32, 1024), (64, 1), (64, 300), (64, 512), (64, 1024)])
+def test_haar_topk_bit_exact(cuda, S, K):
+    import torch
+    faces = np.stack([synth.make_env_faces(S, seed=S * 7 + K, index=e) for e in range(3)])
+    idx, st = _engine().haar_topk(torch.from_numpy(faces).to(cuda), K)
+    ridx, rst = O.haar_topk(faces, K)
+    assert np.array_equal(idx.cpu().numpy(), ridx)
+    assert np.array_equal(st.cpu().numpy().view(np.uint32), rst.view(np.uint32))
+
+
+def test_haar_topk_ties_nan_inf_bit_exact(cuda):
+    import torch
+    S = 8
+    g = np.random.default_rng(11)
+    faces = g.integers(0, 3, size=(4, 6, S, S, 3)).astype(np.float32)  # many equal keys
+    faces[0, 1, 3, 4] = np.nan
+    faces[1, 2, 0, 0, 1] = np.inf
+    faces[2, 5, 7, 7, 2] = -np.inf
+    faces[3] = 1.0                                                     # all-constant faces
+    for K in (1, 17, 64, 6 * S * S):
+        idx, st = _engine().haar_topk(torch.from_numpy(faces).to(cuda), K)
+        ridx, rst = O.haar_topk(faces, K)
+        assert np.array_equal(idx.cpu().numpy(), ridx), K
+        assert np.array_equal(st.cpu().numpy().view(np.uint32), rst.view(np.uint32)), K
+
+
+def test_haar_topk_large_batch(cuda):
+    import torch
+    S, K, E = 64, 300, 96
+    faces = np.stack([synth.make_env_faces(S, seed=3, index=e) for e in range(E)])
+    idx, st = _engine().haar_topk(torch.from_numpy(faces).to(cuda), K)
+    ridx, rst = O.haar_topk(faces, K)
+    assert np.array_equal(idx.cpu().numpy(), ridx)
+    assert np.array_equal(st.cpu().numpy().view(np.uint32), rst.view(np.uint32))
+
+
+def test_haar_topk_rejects_bad_sizes(cuda):
+    import torch
+    eng = _engine()
+    with pytest.raises(eng.NwprtError):
+        eng.haar_topk(torch.zeros((6, 128, 128, 3), device=cuda), 8)
+    with pytest.raises(eng.NwprtError):
+        eng.haar_topk(torch.zeros((6, 16, 16, 3), device=cuda), 1025)
+    with pytest.raises(eng.NwprtError):
+        eng.haar_topk(torch.zeros((6, 2, 2, 3), device=cuda), 25)
+
+
+@pytest.mark.parametrize("S", [1, 16, 64, 128])
+def test_sh_project_vs_f64_oracle(cuda, S):
+    import torch
+    faces = synth.make_env_faces(S, seed=S)
+    L = _engine().sh_project(torch.from_numpy(faces).to(cuda)).cpu().numpy().astype(np.float64)
+    ref, ref_abs = O.sh_project_f64(faces)
+    assert np.all(np.abs(L - ref) <= 1e-5 * ref_abs + 1e-7)
+
+
+@pytest.mark.parametrize("N", [1, 127, 128, 1000, 4097, 128 * 300 + 5])
+@pytest.mark.parametrize("abs_out", [True, False])
+def test_sh_dot_bit_exact(cuda, N, abs_out):
+    import torch
+    T = synth.make_sh_transport(N, seed=N)
+    L = np.random.default_rng(N).normal(size=(81, 3)).astype(np.float32)
+    out = _engine().sh_dot(torch.from_numpy(T).to(cuda), torch.from_numpy(L).to(cuda), abs_out=abs_out)
+    ref = O.sh_dot_f32(T, L, abs_out=abs_out)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_sh_dot_1080p_sampled(cuda):
+    import torch
+    N = 1920 * 1080
+    g = torch.Generator(device=cuda).manual_seed(0)
+    l = torch.floor(torch.sqrt(torch.arange(81, device=cuda, dtype=torch.float32))).clamp_min(1)
+    T = torch.randn((N, 81), generator=g, device=cuda) / (l * l)
+    L = torch.randn((81, 3), generator=g, device=cuda)
+    out = _engine().sh_dot(T, L)
+    rows = np.random.default_rng(0).choice(N, 4096, replace=False)
+    ref = O.sh_dot_f32(T[rows].cpu().numpy(), L.cpu().numpy())
+    assert np.array_equal(out[rows].cpu().numpy().view(np.uint32), ref.view(np.uint32))
