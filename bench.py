@@ -45,7 +45,13 @@ def parse_args():
     ap.add_argument("--fp32-steps", type=int, default=2, help="timed steps of the plain FP32 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--width", type=int, default=1920, help="frame width (profiling runs use smaller cases)")
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--K", type=int, default=300, help="wavelets per pixel")
+    a = ap.parse_args()
+    global WIDTH, HEIGHT, K_WAVELETS
+    WIDTH, HEIGHT, K_WAVELETS = a.width, a.height, a.K
+    return a
 
 
 # ---------------------------------------------------------------------------- helpers
@@ -290,10 +296,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": precision,
             "data": "synthetic: seeded G-buffer, log-normal env map, random-init FP16-rounded weights",
-            "config": {"workload": "relight 1920x1080, K=300 of a 6x64x64 env map, hash 16x2 2^19, "
-                                   "MLPs 32->64x3->64 | 80->64x3->3",
+            "config": {"workload": f"relight {WIDTH}x{HEIGHT}, K={K_WAVELETS} of a 6x64x64 env map, "
+                                   "hash 16x2 2^19, MLPs 32->64x3->64 | 80->64x3->3",
                        "pixels_per_gpu": N, "K": K_WAVELETS, "precision": precision,
-                       "l2": "inputs 209 MB/frame > 126 MB L2 (no flush)",
+                       "l2": f"inputs {h2d / 1e6:.0f} MB/frame vs 126 MB L2 (no flush)",
                        "parallelism": f"request-dp{world}", "step": "TCNNPass_p1 + TCNNPass_p2"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
             "clocks": clocks, "plain_fp32": plain,

@@ -49,8 +49,6 @@ struct EnvEntry {
   float* strength = nullptr;
   float* emb_k = nullptr;     // [K][D], valid when emb_ready
   bool emb_ready = false;
-  uint16_t* tc_table = nullptr;  // tensor-core first-layer table, valid when tc_ready
-  bool tc_ready = false;
 };
 
 struct Frame {
@@ -99,7 +97,6 @@ struct nwprt_ctx {
       dev_free(e.idx);
       dev_free(e.strength);
       dev_free(e.emb_k);
-      dev_free(e.tc_table);
     }
     for (auto& f : frames) dev_free(f.packed);
   }
@@ -164,14 +161,6 @@ void ensure_emb(nwprt_ctx* ctx, EnvEntry& e, cudaStream_t st) {
   e.emb_ready = true;
 }
 
-void ensure_tc_table(nwprt_ctx* ctx, EnvEntry& e, cudaStream_t st) {
-  ensure_emb(ctx, e, st);
-  if (e.tc_ready) return;
-  if (!e.tc_table) e.tc_table = dev_alloc<uint16_t>(tc_env_table_bytes(ctx->dims, e.K) / 2);
-  launch_tc_env_table(ctx->dims, ctx->d_tc_w, e.emb_k, e.K, e.tc_table, st);
-  e.tc_ready = true;
-}
-
 int new_env(nwprt_ctx* ctx, int K) {
   int id = -1;
   for (size_t i = 0; i < ctx->envs.size(); ++i)
@@ -193,7 +182,6 @@ void release_env(EnvEntry& e) {
   dev_free(e.idx);
   dev_free(e.strength);
   dev_free(e.emb_k);
-  dev_free(e.tc_table);
   e = EnvEntry{};
 }
 
@@ -317,10 +305,7 @@ nwprt_status nwprt_load_weights(nwprt_ctx* ctx, const nwprt_weights* w) {
       ctx->d_tc_w = dev_alloc<uint16_t>(tw.size());
       NWPRT_CUDA(cudaMemcpy(ctx->d_tc_w, tw.data(), tw.size() * 2, cudaMemcpyHostToDevice));
     }
-    for (auto& e : ctx->envs) {
-      e.emb_ready = false;
-      e.tc_ready = false;
-    }
+    for (auto& e : ctx->envs) e.emb_ready = false;
     ctx->weights_loaded = true;
   });
 }
@@ -503,10 +488,10 @@ static void relight_many_tc(nwprt_ctx* ctx, const nwprt_request* reqs, int n_req
     need(f.prepared, NWPRT_NOT_READY, "frame was not prepared (call nwprt_prepare first)");
     check_out(r.indirect, "null indirect output");
     check_out(r.with_direct, "null with_direct output");
-    ensure_tc_table(ctx, e, st);
+    ensure_emb(ctx, e, st);
     const int64_t n = (int64_t)f.width * f.height;
     if (n == 0) continue;
-    jobs.push_back(TcJob{f.packed, f.flag, f.direct, e.tc_table, e.strength, e.K, n, r.indirect, r.with_direct});
+    jobs.push_back(TcJob{f.packed, f.flag, f.direct, e.emb_k, e.strength, e.K, n, r.indirect, r.with_direct, 0});
   }
   if (jobs.empty()) return;
   if (ctx->jobs_cap < (int)jobs.size()) {

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <stdexcept>
 #include <string>
@@ -141,19 +142,18 @@ void pack_fp32_weights(const NetDims& d, const float* op, const float* cn,
 bool relight_tc_supported(const NetDims& d, std::string* why);
 size_t tc_weight_bytes(const NetDims& d);
 void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);
-size_t tc_env_table_bytes(const NetDims& d, int K);
-void launch_tc_env_table(const NetDims& d, const uint16_t* tc_weights_dev, const float* emb_k,
-                         int K, uint16_t* table, cudaStream_t st);
+size_t relight_tc_smem_bytes(const NetDims& d);
 struct TcJob {
-  const float* packed;
+  const float* packed;    // [n_px][16]
   const uint8_t* flag;
   const float* direct;
-  const uint16_t* env_table;  // per-k first-layer weights, pre-swizzled BF16
-  const float* strength;
+  const float* emb_k;     // [K][D] FP32 embedding rows of the env's wavelets
+  const float* strength;  // [K][3]
   int K;
   int64_t n_px;
   float* indirect;
   float* with_direct;
+  long long tile_begin;   // first 128-pixel tile of this job in the launch (set by the launcher)
 };
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash,
                        const uint16_t* tc_weights_dev, const TcJob* jobs, int n_jobs,
@@ -187,6 +187,48 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
   }
   if (err) atomicCAS(err, 0u, (uint32_t)kDevWaitTimeout);
   return false;
+}
+
+// ln(x) of a float by the atanh series ln m = 2 (s + s^3/3 + s^5/5 + ...), s = (m-1)/(m+1)
+// (Abramowitz & Stegun 4.1.27), after x = 2^e m with m in [sqrt(1/2), sqrt(2)]; evaluated
+// with IEEE double +, -, *, / and fma in a fixed order and rounded once to float, so host,
+// device and the CPU oracle return the same bits (the correctly rounded logarithm except
+// in rare ties).  Used for the roughness remap log(25r+1)/log(26) (utils_kernels.h:21,39).
+__host__ __device__ inline float float_from_bits(uint32_t u) {
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+__host__ __device__ inline float logf_series(float xf) {
+  if (xf != xf) return xf;
+  if (xf < 0.0f) return float_from_bits(0x7fc00000u);
+  if (xf == 0.0f) return float_from_bits(0xff800000u);
+  if (xf > 3.4028234663852886e38f) return xf;
+  const double x = (double)xf;
+  unsigned long long b;
+  memcpy(&b, &x, 8);
+  int e = (int)((b >> 52) & 0x7ff) - 1023;
+  b = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+  double m;
+  memcpy(&m, &b, 8);
+  if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 23.0;
+  p = fma(p, z, 1.0 / 21.0);
+  p = fma(p, z, 1.0 / 19.0);
+  p = fma(p, z, 1.0 / 17.0);
+  p = fma(p, z, 1.0 / 15.0);
+  p = fma(p, z, 1.0 / 13.0);
+  p = fma(p, z, 1.0 / 11.0);
+  p = fma(p, z, 1.0 / 9.0);
+  p = fma(p, z, 1.0 / 7.0);
+  p = fma(p, z, 1.0 / 5.0);
+  p = fma(p, z, 1.0 / 3.0);
+  p = fma(p, z, 1.0);
+  const double lm = (2.0 * s) * p;
+  return (float)fma((double)e, 0.6931471805599453, lm);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {

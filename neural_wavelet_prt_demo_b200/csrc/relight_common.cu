@@ -3,7 +3,8 @@
 //  * pack_gbuffer: the reference's waveletDataCopy (Renderer/tinycudann/utils_kernels.h:7-49)
 //    without its K-fold replication: one 16-float input row per pixel
 //    (layout prt_globals.h:4-13: pos, normal, reflect, log(25r+1)/log(26), 2kd-1, 2ks-1).
-//    The reference writes 64*K bytes per pixel; this writes 64.
+//    The reference writes 64*K bytes per pixel; this writes 64.  The roughness log uses
+//    logf_series (correctly rounded, identical on host, device and oracle).
 //  * gather_embedding: the per-env half of ptwise_mlt (utils_kernels.h:110-127):
 //    E_k[k][d] = E[d][idx_k] for the env's K selected coefficients, so the fused
 //    transport kernels read one contiguous row per wavelet instead of a strided gather
@@ -23,7 +24,7 @@ __global__ void pack_gbuffer_kernel(int64_t n, const float4* __restrict__ pos,
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const float4 a = pos[p], b = nrm[p], c = refl[p], d = kd[p], e = ks[p];
-  const float r = logf(fmaf(25.f, rough[p], 1.f)) * rgh_den;
+  const float r = logf_series(fmaf(25.f, rough[p], 1.f)) * rgh_den;
   out[p * 4 + 0] = make_float4(a.x, a.y, a.z, b.x);
   out[p * 4 + 1] = make_float4(b.y, b.z, c.x, c.y);
   out[p * 4 + 2] = make_float4(c.z, r, 2.f * d.x - 1.f, 2.f * d.y - 1.f);
@@ -51,8 +52,8 @@ __global__ void gather_embedding_kernel(const float* __restrict__ emb, int D, in
 void launch_pack_gbuffer(const nwprt_gbuffer& g, float* packed, cudaStream_t st) {
   const int64_t n = (int64_t)g.width * g.height;
   if (n == 0) return;
-  // the reference's constant 1/logf(26) (utils_kernels.h:21), evaluated once on the host
-  const float rgh_den = 1.f / logf(25.f + 1.f);
+  // the reference's constant 1/log(26) (utils_kernels.h:21), evaluated once on the host
+  const float rgh_den = 1.f / logf_series(25.f + 1.f);
   const int bs = 256;
   pack_gbuffer_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, st>>>(
       n, (const float4*)g.first_hit_pos, (const float4*)g.world_normal, (const float4*)g.reflect_dir,

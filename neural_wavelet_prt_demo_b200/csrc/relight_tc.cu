@@ -1,22 +1,651 @@
-// tcgen05 tensor-core relight path (BF16 operands, FP32 accumulation in TMEM).
-// Placeholder until the kernel lands: reports the path as unsupported.
+// tcgen05 tensor-core relight kernel: BF16 operands, FP32 accumulation in TMEM.
+//
+// Same computation as the FP32 path (prt_network.h:73-154 + utils_kernels.h:52-127):
+// per pixel p and wavelet k, cp = hash(p) * E[:, idx_k] -> out_prd MLP -> [o || aux]
+// -> cmp_net MLP -> T_k, and sum_k max(L_k * T_k, 0) -- with every dense layer of the
+// 128-pixel x 1-wavelet row block issued as tcgen05.mma (M=128, N<=64, K=16 steps).
+//
+// CTA organisation (one persistent CTA per SM):
+//   warp 0          allocates TMEM; lane 0 issues every MMA and commits it to the
+//                   owning warpgroup's mbarrier.  It serves the warpgroups in whatever
+//                   order they become ready (mbarrier.test_wait probe), so tiles of
+//                   different requests with different K interleave freely.
+//   warps 1..4*NWG  NWG epilogue warpgroups; warpgroup g owns one 128-pixel tile at a time,
+//                   TMEM columns [64g, 64g+64) and its own activation / aux operand
+//                   buffers in shared memory.  Thread (warp w, lane l) owns tile row
+//                   32*(w%4)+l, the TMEM lane it may read.
+// Per layer: MMA -> commit -> epilogue tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 -> st.shared
+// into the next A operand (canonical K-major, no swizzle: 8x16B core matrices,
+// LBO = 128 B between K chunks, SBO = 1024 B between 8-row groups) -> fence.proxy.async
+// -> mbarrier arrive.  The last layer's epilogue reads T_k (3 columns), does the clamped
+// Kahan sum and writes the next wavelet's first-layer operand hash(p) * E_k+1 (FP32
+// product, rounded once to BF16), so the transport never leaves the SM.
+// Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
+// kDevWaitTimeout in the error word and unwinds.
+#include <cmath>
+#include <cstring>
+
 #include "nwprt_internal.cuh"
 
 namespace nwprt {
+namespace {
 
-bool relight_tc_supported(const NetDims&, std::string* why) {
-  if (why) *why = "tensor-core path not built";
+constexpr int kNWG = 4;                    // epilogue warpgroups per CTA
+constexpr int kThreads = 32 + 128 * kNWG;  // + MMA warp
+constexpr int kTile = 128;                 // pixels per tile (MMA M)
+constexpr int kActBytes = kTile * 64 * 2;  // 128 x 64 bf16
+constexpr int kAuxBytes = kTile * 16 * 2;  // 128 x 16 bf16
+constexpr int kMaxTcLayers = 12;
+constexpr int kTmemCols = 256;
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+struct TcLayer {
+  uint32_t b_off;  // byte offset of B (N x K, canonical K-major) in the weight blob
+  uint32_t b_sbo;  // B stride between 8-row groups (= K * 16 bytes)
+  int k;           // reduction length (multiple of 16)
+  int n;           // output width: 32 or 64 (hidden), 16 (final)
+  int relu;
+  int aux;         // also accumulate aux (K=16) x aux block of B at aux_off
+  uint32_t aux_off;
+  int fin;         // last layer: columns 0..2 are T_k
+};
+
+struct TcParams {
+  HashLevels hl;
+  const float* hash;
+  const uint4* wblob;
+  uint32_t wblob_bytes;
+  TcLayer layers[kMaxTcLayers];
+  int n_layers;
+  int enc_dims;  // D, multiple of 16, <= 64
+  const TcJob* jobs;
+  int n_jobs;
+  long long total_tiles;
+  int kahan, clamp;
+  uint32_t* err;
+};
+
+// ------------------------------------------------------------------ PTX wrappers
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Wait for the phase with `parity`, bounded by kWaitNs of wall time.
+__device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err) {
+  const uint32_t a = smem_u32(bar);
+  if (mbar_try(a, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 1; it < (1u << 30); ++it) {
+    if (mbar_try(a, parity)) return true;
+    if ((it & 255u) == 0 && globaltimer() - t0 > kWaitNs) break;
+  }
+  atomicCAS(err, 0u, (uint32_t)kDevWaitTimeout);
   return false;
 }
-size_t tc_weight_bytes(const NetDims&) { return 0; }
-void pack_tc_weights(const NetDims&, const float*, const float*, std::vector<uint16_t>* out) { out->clear(); }
-size_t tc_env_table_bytes(const NetDims&, int) { return 0; }
-void launch_tc_env_table(const NetDims&, const uint16_t*, const float*, int, uint16_t*, cudaStream_t) {
-  fail(NWPRT_UNSUPPORTED, "tensor-core path not built");
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
 }
-void launch_relight_tc(const NetDims&, const HashLevels&, const float*, const uint16_t*, const TcJob*, int,
-                       TcJob*, int, int, uint32_t*, cudaStream_t) {
-  fail(NWPRT_UNSUPPORTED, "tensor-core path not built");
+
+// kind::f16 instruction descriptor: D=F32, A=B=BF16, both K-major, M=128.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+#define NWPRT_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
+                    "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : NWPRT_R8(0), NWPRT_R8(8), NWPRT_R8(16), NWPRT_R8(24)
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+__device__ __forceinline__ uint32_t pack_bf16_relu(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
+               : "memory");
+}
+
+// Byte offset of (row, 16-byte K chunk) in a canonical no-swizzle K-major tile whose
+// 8-row groups are `sbo` bytes apart.
+__device__ __forceinline__ uint32_t core_off(int row, int chunk, uint32_t sbo) {
+  return (uint32_t)(row >> 3) * sbo + (uint32_t)chunk * 128u + (uint32_t)(row & 7) * 16u;
+}
+
+// Converts 32 TMEM columns (FP32 bit patterns) to 4 BF16 chunks of the next A operand.
+template <bool RELU>
+__device__ __forceinline__ void store_chunks32(const uint32_t (&v)[32], uint32_t act_row_base, int chunk0) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint32_t q[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float lo = __uint_as_float(v[c * 8 + 2 * j]), hi = __uint_as_float(v[c * 8 + 2 * j + 1]);
+      q[j] = RELU ? pack_bf16_relu(lo, hi) : pack_bf16(lo, hi);
+    }
+    st_shared_v4(act_row_base + (uint32_t)(chunk0 + c) * 128u, q[0], q[1], q[2], q[3]);
+  }
+}
+
+// Hash-grid encoding into registers (same arithmetic as the FP32 path).
+template <int DMAX>
+__device__ __forceinline__ void hash_encode_regs(const HashLevels& hl, const float* __restrict__ table,
+                                                 float px, float py, float pz, float (&enc)[DMAX]) {
+  const float p[3] = {fminf(fmaxf(px, 0.f), 1.f), fminf(fmaxf(py, 0.f), 1.f), fminf(fmaxf(pz, 0.f), 1.f)};
+#pragma unroll
+  for (int i = 0; i < DMAX; ++i) enc[i] = 0.f;
+#pragma unroll
+  for (int l = 0; l < DMAX / 2; ++l) {
+    if (l < hl.n_levels) {
+      const int N = hl.res[l];
+      uint32_t i0[3];
+      float w[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float xl = __fmul_rn(p[d], (float)N);
+        int i = (int)floorf(xl);
+        if (i > N - 1) i = N - 1;
+        i0[d] = (uint32_t)i;
+        w[d] = __fsub_rn(xl, (float)i);
+      }
+      const uint32_t N1 = (uint32_t)N + 1u;
+      const bool dense = (hl.dense_mask >> l) & 1u;
+      const uint32_t T = hl.size[l];
+      const float2* lvl = reinterpret_cast<const float2*>(table) + hl.offset[l];
+      float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const uint32_t bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+        const float wx = bx ? w[0] : __fsub_rn(1.f, w[0]);
+        const float wy = by ? w[1] : __fsub_rn(1.f, w[1]);
+        const float wz = bz ? w[2] : __fsub_rn(1.f, w[2]);
+        const float wc = __fmul_rn(__fmul_rn(wx, wy), wz);
+        const uint32_t x = i0[0] + bx, y = i0[1] + by, z = i0[2] + bz;
+        const uint32_t e = dense ? x + y * N1 + z * N1 * N1
+                                 : ((x ^ (y * 2654435761u) ^ (z * 805459861u)) & (T - 1u));
+        const float2 v = __ldg(lvl + e);
+        a0 = fmaf(wc, v.x, a0);
+        a1 = fmaf(wc, v.y, a1);
+      }
+      enc[2 * l] = a0;
+      enc[2 * l + 1] = a1;
+    }
+  }
+}
+
+// First-layer operand of wavelet k: row = hash(p) * E_k, rounded once to BF16.
+template <int DMAX>
+__device__ __forceinline__ void store_cp(const float (&enc)[DMAX], const float* __restrict__ ek, int D,
+                                         uint32_t act_row_base) {
+#pragma unroll
+  for (int c = 0; c < DMAX / 8; ++c) {
+    if (c * 8 < D) {
+      const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
+      const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
+      st_shared_v4(act_row_base + (uint32_t)c * 128u,
+                   pack_bf16(__fmul_rn(enc[c * 8 + 0], e0.x), __fmul_rn(enc[c * 8 + 1], e0.y)),
+                   pack_bf16(__fmul_rn(enc[c * 8 + 2], e0.z), __fmul_rn(enc[c * 8 + 3], e0.w)),
+                   pack_bf16(__fmul_rn(enc[c * 8 + 4], e1.x), __fmul_rn(enc[c * 8 + 5], e1.y)),
+                   pack_bf16(__fmul_rn(enc[c * 8 + 6], e1.z), __fmul_rn(enc[c * 8 + 7], e1.w)));
+    }
+  }
+}
+
+__device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long tile) {
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct __align__(8) TcBarriers {
+  uint64_t acc_full[kNWG];   // MMA -> epilogue: accumulator of the current layer ready
+  uint64_t act_ready[kNWG];  // epilogue -> MMA: next A operand written, TMEM drained (4 arrivals)
+  uint64_t done;             // final commit before TMEM is released
+  uint32_t tmem_base;
+};
+
+template <int DMAX>
+__global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_constant__ TcParams p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* wsm = smem;                                            // weight blob
+  uint8_t* act = smem + ((p.wblob_bytes + 1023u) & ~1023u);       // [kNWG][kActBytes]
+  uint8_t* aux = act + kNWG * kActBytes;                          // [kNWG][kAuxBytes]
+  TcBarriers* bars = reinterpret_cast<TcBarriers*>(aux + kNWG * kAuxBytes);
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+
+  // ---- weights -> shared memory (generic proxy), barriers, TMEM
+  for (uint32_t i = tid; i < p.wblob_bytes / 16u; i += kThreads)
+    reinterpret_cast<uint4*>(wsm)[i] = __ldg(p.wblob + i);
+  if (tid == 0) {
+    for (int g = 0; g < kNWG; ++g) {
+      mbar_init(&bars->acc_full[g], 1);
+      mbar_init(&bars->act_ready[g], 4);
+    }
+    mbar_init(&bars->done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&bars->tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = bars->tmem_base;
+  const long long stride = (long long)gridDim.x * kNWG;
+
+  if (warp == 0) {
+    // ================================================================ MMA issuer
+    if (lane == 0) {
+      const uint32_t wbase = smem_u32(wsm);
+      long long tile[kNWG];
+      int K[kNWG], k[kNWG], l[kNWG];
+      uint32_t ph[kNWG];
+      int live = 0;
+      for (int g = 0; g < kNWG; ++g) {
+        tile[g] = (long long)blockIdx.x * kNWG + g;
+        k[g] = 0;
+        l[g] = 0;
+        ph[g] = 0;
+        K[g] = 0;
+        if (tile[g] < p.total_tiles) {
+          K[g] = p.jobs[find_job(p.jobs, p.n_jobs, tile[g])].K;
+          ++live;
+        }
+      }
+      uint64_t idle_since = 0;
+      bool failed = false;
+      while (live > 0 && !failed) {
+        bool progressed = false;
+        for (int g = 0; g < kNWG; ++g) {
+          if (tile[g] >= p.total_tiles) continue;
+          if (!mbar_test(smem_u32(&bars->act_ready[g]), ph[g])) continue;
+          ph[g] ^= 1u;
+          progressed = true;
+          tc_fence_after();
+          const TcLayer& L = p.layers[l[g]];
+          const uint32_t a_base = smem_u32(act + g * kActBytes);
+          const uint32_t d = tmem + (uint32_t)(g * 64);
+          const uint32_t id = idesc_bf16(L.n);
+          for (int s = 0; s < L.k / 16; ++s) {
+            const uint64_t ad = smem_desc(a_base + (uint32_t)s * 256u, 128u, 1024u);
+            const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
+            mma_bf16(d, ad, bd, id, s > 0 ? 1u : 0u);
+          }
+          if (L.aux) {
+            const uint64_t ad = smem_desc(smem_u32(aux + g * kAuxBytes), 128u, 256u);
+            const uint64_t bd = smem_desc(wbase + L.aux_off, 128u, 256u);
+            mma_bf16(d, ad, bd, id, 1u);
+          }
+          mma_commit(&bars->acc_full[g]);
+          if (++l[g] == p.n_layers) {
+            l[g] = 0;
+            if (++k[g] == K[g]) {
+              k[g] = 0;
+              tile[g] += stride;
+              if (tile[g] < p.total_tiles) K[g] = p.jobs[find_job(p.jobs, p.n_jobs, tile[g])].K;
+              else --live;
+            }
+          }
+        }
+        if (progressed) {
+          idle_since = 0;
+        } else {
+          const uint64_t now = globaltimer();
+          if (idle_since == 0) idle_since = now;
+          else if (now - idle_since > kWaitNs) {
+            atomicCAS(p.err, 0u, (uint32_t)kDevWaitTimeout);
+            failed = true;
+          }
+        }
+      }
+      // every issued MMA has completed before TMEM is released
+      mma_commit(&bars->done);
+      wait_bounded(&bars->done, 0, p.err);
+    }
+  } else {
+    // ================================================================ epilogue warpgroups
+    const int g = (warp - 1) >> 2;
+    const int q = warp & 3;                       // TMEM lane quarter this warp may read
+    const int row = q * 32 + lane;                // tile row = pixel within the tile
+    const uint32_t act_row = smem_u32(act + g * kActBytes) + core_off(row, 0, 1024u);
+    const uint32_t aux_row = smem_u32(aux + g * kAuxBytes) + core_off(row, 0, 256u);
+    const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * 64);
+    uint32_t acc_ph = 0;
+    bool ok = true;
+    for (long long t = (long long)blockIdx.x * kNWG + g; t < p.total_tiles && ok; t += stride) {
+      const TcJob& J = p.jobs[find_job(p.jobs, p.n_jobs, t)];
+      const long long px = (t - J.tile_begin) * kTile + row;
+      const bool valid = px < J.n_px;
+      float enc[DMAX];
+      bool active = false;
+      if (valid) {
+        const float4* pr = reinterpret_cast<const float4*>(J.packed) + px * 4;
+        const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3);
+        hash_encode_regs<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, enc);
+        active = J.flag[px] != 0;
+        // aux operand: the 13 remapped G-buffer values followed by ones
+        st_shared_v4(aux_row, pack_bf16(r0.w, r1.x), pack_bf16(r1.y, r1.z), pack_bf16(r1.w, r2.x),
+                     pack_bf16(r2.y, r2.z));
+        st_shared_v4(aux_row + 128u, pack_bf16(r2.w, r3.x), pack_bf16(r3.y, r3.z), pack_bf16(r3.w, 1.f),
+                     pack_bf16(1.f, 1.f));
+      } else {
+#pragma unroll
+        for (int i = 0; i < DMAX; ++i) enc[i] = 0.f;
+        st_shared_v4(aux_row, 0, 0, 0, 0);
+        st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
+      }
+      store_cp<DMAX>(enc, J.emb_k, p.enc_dims, act_row);
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bars->act_ready[g]);
+      float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+      for (int k = 0; k < J.K && ok; ++k) {
+        for (int li = 0; li < p.n_layers; ++li) {
+          const TcLayer& L = p.layers[li];
+          // warp-uniform outcome: tcgen05.ld below is .sync.aligned
+          ok = __all_sync(0xffffffffu, wait_bounded(&bars->acc_full[g], acc_ph, p.err));
+          if (!ok) break;
+          acc_ph ^= 1u;
+          tc_fence_after();
+          if (!L.fin) {
+            uint32_t v[32];
+            tmem_ld32(taddr, v);
+            tmem_wait_ld();
+            if (L.relu) store_chunks32<true>(v, act_row, 0);
+            else store_chunks32<false>(v, act_row, 0);
+            if (L.n > 32) {
+              tmem_ld32(taddr + 32u, v);
+              tmem_wait_ld();
+              if (L.relu) store_chunks32<true>(v, act_row, 4);
+              else store_chunks32<false>(v, act_row, 4);
+            }
+          } else {
+            uint32_t v[4];
+            tmem_ld4(taddr, v);
+            tmem_wait_ld();
+            const float* Lk = J.strength + (size_t)k * 3;
+            float t0 = __fmul_rn(__ldg(Lk + 0), __uint_as_float(v[0]));
+            float t1 = __fmul_rn(__ldg(Lk + 1), __uint_as_float(v[1]));
+            float t2 = __fmul_rn(__ldg(Lk + 2), __uint_as_float(v[2]));
+            if (p.clamp) { t0 = fmaxf(t0, 0.f); t1 = fmaxf(t1, 0.f); t2 = fmaxf(t2, 0.f); }
+            if (p.kahan) {
+              float y, z;
+              y = __fsub_rn(t0, c0); z = __fadd_rn(s0, y); c0 = __fsub_rn(__fsub_rn(z, s0), y); s0 = z;
+              y = __fsub_rn(t1, c1); z = __fadd_rn(s1, y); c1 = __fsub_rn(__fsub_rn(z, s1), y); s1 = z;
+              y = __fsub_rn(t2, c2); z = __fadd_rn(s2, y); c2 = __fsub_rn(__fsub_rn(z, s2), y); s2 = z;
+            } else {
+              s0 = __fadd_rn(s0, t0); s1 = __fadd_rn(s1, t1); s2 = __fadd_rn(s2, t2);
+            }
+            if (k + 1 < J.K) store_cp<DMAX>(enc, J.emb_k + (size_t)(k + 1) * p.enc_dims, p.enc_dims, act_row);
+          }
+          const bool last = L.fin && k + 1 == J.K;  // the next tile's set-up arrives instead
+          if (!last) {
+            tc_fence_before();
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars->act_ready[g]);
+          } else {
+            tc_fence_before();
+          }
+        }
+      }
+      if (valid && ok) {
+        float4 ind = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (active) ind = make_float4(s0, s1, s2, 1.f);
+        const float4 dl = __ldg(reinterpret_cast<const float4*>(J.direct) + px);
+        reinterpret_cast<float4*>(J.indirect)[px] = ind;
+        reinterpret_cast<float4*>(J.with_direct)[px] =
+            make_float4(__fadd_rn(ind.x, dl.x), __fadd_rn(ind.y, dl.y), __fadd_rn(ind.z, dl.z), 1.f);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                 : "memory");
+}
+
+// ------------------------------------------------------------------ host-side packing
+uint16_t to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+int pad16(int x) { return (x + 15) & ~15; }
+
+// Writes the N x K (row-major [out][in]) block src[:, col0:col0+kc] as a canonical
+// K-major tile of np x kp BF16 (zero padded) at byte offset `off` of the blob.
+void put_b(std::vector<uint16_t>* blob, size_t off, const float* src, int n, int k_total, int col0, int kc,
+           int np, int kp) {
+  const size_t need = off / 2 + (size_t)np * kp;
+  if (blob->size() < need) blob->resize(need, 0);
+  const uint32_t sbo = (uint32_t)kp * 16u;
+  for (int r = 0; r < np; ++r)
+    for (int c = 0; c < kp; ++c) {
+      const float v = (r < n && c < kc) ? src[(size_t)r * k_total + col0 + c] : 0.f;
+      const size_t byte = off + (size_t)(r >> 3) * sbo + (size_t)(c >> 3) * 128 + (size_t)(r & 7) * 16 +
+                          (size_t)(c & 7) * 2;
+      (*blob)[byte / 2] = to_bf16(v);
+    }
+}
+
+struct Plan {
+  TcLayer layers[kMaxTcLayers];
+  int n_layers = 0;
+  std::vector<uint16_t> blob;
+};
+
+bool plan_supported(const NetDims& d, std::string* why) {
+  auto no = [&](const char* m) { if (why) *why = m; return false; };
+  if (d.aux_width != 16) return no("tensor-core path needs a 16-wide aux encoding");
+  if (d.enc_dims() % 16 || d.enc_dims() > 32) return no("tensor-core path needs 16 or 32 hash features");
+  if (d.op_out > 64) return no("tensor-core path needs out_prd outputs <= 64");
+  if (d.op_nl + d.cn_nl > kMaxTcLayers) return no("too many layers for the tensor-core path");
+  for (int i = 0; i < d.op_nl; ++i)
+    if (pad16(d.op_outs[i]) > 64 || (i > 0 && pad16(d.op_in[i]) > 64)) return no("tensor-core path needs widths <= 64");
+  for (int i = 1; i < d.cn_nl; ++i)
+    if (pad16(d.cn_in[i]) > 64 || pad16(d.cn_outs[i]) > 64) return no("tensor-core path needs widths <= 64");
+  if (pad16(d.cn_outs[0]) > 64) return no("tensor-core path needs widths <= 64");
+  for (int i = 0; i < d.op_nl; ++i)
+    if (pad16(d.op_outs[i]) == 48 || pad16(d.op_outs[i]) == 16) return no("hidden widths must pad to 32 or 64");
+  for (int i = 0; i + 1 < d.cn_nl; ++i)
+    if (pad16(d.cn_outs[i]) == 48 || pad16(d.cn_outs[i]) == 16) return no("hidden widths must pad to 32 or 64");
+  return true;
+}
+
+Plan make_plan(const NetDims& d, const float* op, const float* cn) {
+  Plan P;
+  size_t off = 0;
+  auto add = [&](const float* W, int n, int k_total, int col0, int kc, bool relu, bool fin) {
+    TcLayer L{};
+    const int np = fin ? 16 : pad16(n), kp = pad16(kc);
+    L.b_off = (uint32_t)off;
+    L.b_sbo = (uint32_t)kp * 16u;
+    L.k = kp;
+    L.n = np;
+    L.relu = relu;
+    L.fin = fin;
+    if (op || cn) put_b(&P.blob, off, W, n, k_total, col0, kc, np, kp);
+    off += (size_t)np * kp * 2;
+    off = (off + 127) & ~size_t(127);
+    P.layers[P.n_layers++] = L;
+    return P.n_layers - 1;
+  };
+  const float* w = op;
+  for (int i = 0; i < d.op_nl; ++i) {
+    add(w, d.op_outs[i], d.op_in[i], 0, d.op_in[i], i + 1 < d.op_nl, false);
+    if (w) w += (size_t)d.op_in[i] * d.op_outs[i];
+  }
+  w = cn;
+  for (int i = 0; i < d.cn_nl; ++i) {
+    const bool fin = i + 1 == d.cn_nl;
+    if (i == 0) {
+      const int li = add(w, d.cn_outs[0], d.cn_in[0], 0, d.op_out, !fin, fin);
+      // aux block: columns [op_out, op_out + 16) of cmp_net's first layer
+      P.layers[li].aux = 1;
+      P.layers[li].aux_off = (uint32_t)off;
+      const int np = fin ? 16 : pad16(d.cn_outs[0]);
+      if (op || cn) put_b(&P.blob, off, w, d.cn_outs[0], d.cn_in[0], d.op_out, 16, np, 16);
+      off += (size_t)np * 16 * 2;
+      off = (off + 127) & ~size_t(127);
+    } else {
+      add(w, d.cn_outs[i], d.cn_in[i], 0, d.cn_in[i], !fin, fin);
+    }
+    if (w) w += (size_t)d.cn_in[i] * d.cn_outs[i];
+  }
+  P.blob.resize(off / 2, 0);
+  return P;
+}
+
+}  // namespace
+
+bool relight_tc_supported(const NetDims& d, std::string* why) { return plan_supported(d, why); }
+
+size_t tc_weight_bytes(const NetDims& d) { return make_plan(d, nullptr, nullptr).blob.size() * 2; }
+
+void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out) {
+  *out = make_plan(d, op, cn).blob;
+}
+
+size_t relight_tc_smem_bytes(const NetDims& d) {
+  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * (kActBytes + kAuxBytes) +
+         sizeof(TcBarriers);
+}
+
+void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const uint16_t* tc_weights_dev,
+                       const TcJob* jobs, int n_jobs, TcJob* jobs_dev, int kahan, int clamp, uint32_t* err,
+                       cudaStream_t st) {
+  std::string why;
+  if (!plan_supported(d, &why)) fail(NWPRT_UNSUPPORTED, why);
+  if (n_jobs <= 0) return;
+  Plan P = make_plan(d, nullptr, nullptr);
+  TcParams p{};
+  p.hl = hl;
+  p.hash = hash;
+  p.wblob = reinterpret_cast<const uint4*>(tc_weights_dev);
+  p.wblob_bytes = (uint32_t)(P.blob.size() * 2);
+  std::memcpy(p.layers, P.layers, sizeof(P.layers));
+  p.n_layers = P.n_layers;
+  p.enc_dims = d.enc_dims();
+  p.n_jobs = n_jobs;
+  p.kahan = kahan;
+  p.clamp = clamp;
+  p.err = err;
+  // tile prefix over the jobs, then one copy of the job table (stream ordered)
+  std::vector<TcJob> J(jobs, jobs + n_jobs);
+  long long tiles = 0;
+  for (auto& j : J) {
+    j.tile_begin = tiles;
+    tiles += (j.n_px + kTile - 1) / kTile;
+  }
+  if (tiles == 0) return;
+  p.total_tiles = tiles;
+  p.jobs = jobs_dev;
+  NWPRT_CUDA(cudaMemcpyAsync(jobs_dev, J.data(), sizeof(TcJob) * J.size(), cudaMemcpyHostToDevice, st));
+  int dev = 0, sms = 0, max_smem = 0;
+  NWPRT_CUDA(cudaGetDevice(&dev));
+  NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  NWPRT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t smem = relight_tc_smem_bytes(d);
+  if (smem > (size_t)max_smem) fail(NWPRT_UNSUPPORTED, "tensor-core relight: shared memory budget exceeded");
+  const long long groups = (tiles + kNWG - 1) / kNWG;
+  const int grid = (int)(groups < sms ? groups : sms);
+  if (d.enc_dims() <= 16) {
+    auto k = relight_tc_kernel<16>;
+    NWPRT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kThreads, smem, st>>>(p);
+  } else {
+    auto k = relight_tc_kernel<32>;
+    NWPRT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kThreads, smem, st>>>(p);
+  }
+  NWPRT_CUDA(cudaGetLastError());
 }
 
 }  // namespace nwprt

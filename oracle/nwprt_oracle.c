@@ -265,11 +265,49 @@ void orc_sh_dot_f64(const float* T, int64_t N, int nc, const double* L, int abs_
 /* Relight                                                                   */
 /* ------------------------------------------------------------------------ */
 
+/* ln(x) of a float, evaluated in double by the atanh series
+ *   ln m = 2 artanh((m-1)/(m+1)) = 2 (s + s^3/3 + s^5/5 + ...)   (Abramowitz & Stegun 4.1.27)
+ * after the reduction x = 2^e m, m in [sqrt(1/2), sqrt(2)], and rounded once to float.
+ * Only IEEE double +, -, *, / and fma in a fixed order, so the GPU's copy of this
+ * routine (relight_common.cu) returns the same bits; its result is the correctly rounded
+ * float logarithm except in rare ties.  Used for the roughness remap in place of logf,
+ * whose last bit differs between C libraries and the GPU. */
+float orc_logf_series(float xf) {
+  if (xf != xf) return xf;
+  if (xf < 0.0f) return NAN;
+  if (xf == 0.0f) return -INFINITY;
+  if (isinf(xf)) return xf;
+  double x = (double)xf;
+  uint64_t b;
+  memcpy(&b, &x, 8);
+  int e = (int)((b >> 52) & 0x7ff) - 1023;
+  b = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+  double m;
+  memcpy(&m, &b, 8);
+  if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 23.0;
+  p = fma(p, z, 1.0 / 21.0);
+  p = fma(p, z, 1.0 / 19.0);
+  p = fma(p, z, 1.0 / 17.0);
+  p = fma(p, z, 1.0 / 15.0);
+  p = fma(p, z, 1.0 / 13.0);
+  p = fma(p, z, 1.0 / 11.0);
+  p = fma(p, z, 1.0 / 9.0);
+  p = fma(p, z, 1.0 / 7.0);
+  p = fma(p, z, 1.0 / 5.0);
+  p = fma(p, z, 1.0 / 3.0);
+  p = fma(p, z, 1.0);
+  const double lm = (2.0 * s) * p;
+  return (float)fma((double)e, 0.6931471805599453, lm);
+}
+
 /* The reference's per-pixel 16-float input row (waveletDataCopy,
  * utils_kernels.h:7-49; layout prt_globals.h:4-13):
  * pos(3) normal(3) reflect(3) log(25r+1)/log(26) 2kd-1(3) 2ks-1(3). */
 void orc_remap_f32(const orc_gbuf* g, int64_t px, float row[16]) {
-  const float rgh_den = 1.f / logf(25.f + 1.f);
+  const float rgh_den = 1.f / orc_logf_series(25.f + 1.f);
   for (int i = 0; i < 3; ++i) {
     row[0 + i] = g->pos[px * 4 + i];
     row[3 + i] = g->normal[px * 4 + i];
@@ -277,7 +315,7 @@ void orc_remap_f32(const orc_gbuf* g, int64_t px, float row[16]) {
     row[10 + i] = 2.f * g->kd[px * 4 + i] - 1.f;
     row[13 + i] = 2.f * g->ks[px * 4 + i] - 1.f;
   }
-  row[9] = logf(fmaf(25.f, g->roughness[px], 1.f)) * rgh_den;
+  row[9] = orc_logf_series(fmaf(25.f, g->roughness[px], 1.f)) * rgh_den;
 }
 
 static float clamp01f(float x) { return fminf(fmaxf(x, 0.f), 1.f); }

@@ -75,6 +75,7 @@ void orc_sh_dot_f32(const float* T, int64_t N, int nc, const float* L, int abs_o
 void orc_sh_dot_f64(const float* T, int64_t N, int nc, const double* L, int abs_out, double* out3);
 
 /* ---- relight pieces ---- */
+float orc_logf_series(float x);
 void orc_remap_f32(const orc_gbuf* g, int64_t px, float row[16]);
 void orc_hash_encode_f32(const orc_net* net, const float* hash, const float pos[3], float* out);
 void orc_hash_encode_f64(const orc_net* net, const float* hash, const float pos[3], double* out);

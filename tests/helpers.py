@@ -44,3 +44,16 @@ def psnr(x, ref):
     if mse == 0:
         return float("inf")
     return 10.0 * np.log10(peak * peak / mse)
+
+
+def bits_equal(a, b) -> bool:
+    """Bitwise float32 equality, except that any NaN equals any NaN (x86 and the GPU
+    produce different NaN payloads for the same invalid operation)."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    if a.shape != b.shape:
+        return False
+    na, nb = np.isnan(a), np.isnan(b)
+    if not np.array_equal(na, nb):
+        return False
+    return bool(np.array_equal(a[~na].view(np.uint32), b[~nb].view(np.uint32)))

