@@ -2,26 +2,27 @@
 //
 // Same computation as the FP32 path (prt_network.h:73-154 + utils_kernels.h:52-127):
 // per pixel p and wavelet k, cp = hash(p) * E[:, idx_k] -> out_prd MLP -> [o || aux]
-// -> cmp_net MLP -> T_k, and sum_k max(L_k * T_k, 0) -- with every dense layer of the
-// 128-pixel x 1-wavelet row block issued as tcgen05.mma (M=128, N<=64, K=16 steps).
+// -> cmp_net MLP -> T_k, and sum_k max(L_k * T_k, 0).  Every hidden dense layer of a
+// 128-pixel x 1-wavelet row block is issued as tcgen05.mma (M=128, N<=64, K=16 steps);
+// the final 3-output layer runs in FP32 on the CUDA cores inside the epilogue of the
+// layer before it, straight from the FP32 accumulator.
 //
-// CTA organisation (one persistent CTA per SM):
-//   warp 0          allocates TMEM; lane 0 issues every MMA and commits it to the
-//                   owning warpgroup's mbarrier.  It serves the warpgroups in whatever
-//                   order they become ready (mbarrier.test_wait probe), so tiles of
-//                   different requests with different K interleave freely.
-//   warps 1..4*NWG  NWG epilogue warpgroups; warpgroup g owns one 128-pixel tile at a time,
-//                   TMEM columns [64g, 64g+64) and its own activation / aux operand
-//                   buffers in shared memory.  Thread (warp w, lane l) owns tile row
-//                   32*(w%4)+l, the TMEM lane it may read.
-// Per layer: MMA -> commit -> epilogue tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 -> st.shared
-// into the next A operand (canonical K-major, no swizzle: 8x16B core matrices,
+// Measured on B200: a tcgen05.mma costs >= ~60 cycles whatever N <= 64 (N=128 takes 64,
+// N=256 128), so these 64-wide layers are issue-bound at ~53% of the tensor peak; the
+// kernel's job is to keep that issue slot busy.  Organisation (one persistent CTA per SM):
+//   kNWG warpgroups x kTPW tiles: warpgroup g keeps kTPW 128-pixel tiles in flight, each
+//   with its own 64 TMEM columns and its own A-operand buffers in shared memory.  While
+//   the tensor core runs one tile's layer the warpgroup drains another tile's accumulator.
+//   Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may read.
+// Per layer of a tile: wait acc barrier -> tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 ->
+// st.shared into the next A operand (canonical K-major, no swizzle: 8x16B core matrices,
 // LBO = 128 B between K chunks, SBO = 1024 B between 8-row groups) -> fence.proxy.async
-// -> mbarrier arrive.  The last layer's epilogue reads T_k (3 columns), does the clamped
-// Kahan sum and writes the next wavelet's first-layer operand hash(p) * E_k+1 (FP32
-// product, rounded once to BF16), so the transport never leaves the SM.
-// Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
-// kDevWaitTimeout in the error word and unwinds.
+// -> warpgroup barrier (bar.red.and carrying the "no timeout" vote) -> one elected thread
+// issues the next layer's MMAs and commits them to the tile's barrier.
+// The final layer's epilogue forms T_k = V_last relu(h) in FP32, does the clamped Kahan
+// sum and writes the next wavelet's first-layer operand hash(p) * E_k+1, so the
+// transport never leaves the SM.  Every wait is bounded by %globaltimer (2 s); on expiry
+// the kernel records kDevWaitTimeout and the whole warpgroup unwinds together.
 #include <cmath>
 #include <cstring>
 
@@ -30,24 +31,28 @@
 namespace nwprt {
 namespace {
 
-constexpr int kNWG = 4;                    // epilogue warpgroups per CTA
-constexpr int kThreads = 32 + 128 * kNWG;  // + MMA warp
+constexpr int kNWG = 4;                    // warpgroups per CTA
+constexpr int kTPW = 2;                    // tiles in flight per warpgroup
+constexpr int kThreads = 128 * kNWG;
+constexpr int kSlots = kNWG * kTPW;
 constexpr int kTile = 128;                 // pixels per tile (MMA M)
 constexpr int kActBytes = kTile * 64 * 2;  // 128 x 64 bf16
 constexpr int kAuxBytes = kTile * 16 * 2;  // 128 x 16 bf16
 constexpr int kMaxTcLayers = 12;
-constexpr int kTmemCols = 256;
+constexpr int kTmemCols = 512;
+constexpr int kVlastFloats = 3 * 64;
 constexpr uint64_t kWaitNs = 2000000000ull;
+static_assert(kSlots * 64 <= kTmemCols, "TMEM budget");
 
 struct TcLayer {
   uint32_t b_off;  // byte offset of B (N x K, canonical K-major) in the weight blob
   uint32_t b_sbo;  // B stride between 8-row groups (= K * 16 bytes)
   int k;           // reduction length (multiple of 16)
-  int n;           // output width: 32 or 64 (hidden), 16 (final)
+  int n;           // output width: 32 or 64
   int relu;
   int aux;         // also accumulate aux (K=16) x aux block of B at aux_off
   uint32_t aux_off;
-  int fin;         // last layer: columns 0..2 are T_k
+  int fin;         // the epilogue forms T_k = V_last relu(h) from this layer's output
 };
 
 struct TcParams {
@@ -55,9 +60,10 @@ struct TcParams {
   const float* hash;
   const uint4* wblob;
   uint32_t wblob_bytes;
+  uint32_t vlast_off;  // byte offset of V_last (FP32 [3][64]) in the blob
   TcLayer layers[kMaxTcLayers];
   int n_layers;
-  int enc_dims;  // D, multiple of 16, <= 64
+  int enc_dims;  // D, multiple of 16, <= 32
   const TcJob* jobs;
   int n_jobs;
   long long total_tiles;
@@ -70,18 +76,6 @@ __device__ __forceinline__ uint64_t globaltimer() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
-}
-
-__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return done != 0;
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
@@ -107,6 +101,20 @@ __device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity, uin
   }
   atomicCAS(err, 0u, (uint32_t)kDevWaitTimeout);
   return false;
+}
+
+// Warpgroup barrier (named barrier 1+g, 128 threads) that also ANDs a predicate.
+__device__ __forceinline__ bool wg_barrier_and(int g, bool pred) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)pred), "r"(1 + g)
+      : "memory");
+  return out != 0;
 }
 
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
@@ -155,12 +163,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
       : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(taddr));
-}
-
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   uint32_t d;
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
@@ -171,6 +173,8 @@ __device__ __forceinline__ uint32_t pack_bf16_relu(float lo, float hi) {
   asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
+__device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
@@ -183,7 +187,7 @@ __device__ __forceinline__ uint32_t core_off(int row, int chunk, uint32_t sbo) {
   return (uint32_t)(row >> 3) * sbo + (uint32_t)chunk * 128u + (uint32_t)(row & 7) * 16u;
 }
 
-// Converts 32 TMEM columns (FP32 bit patterns) to 4 BF16 chunks of the next A operand.
+// 32 TMEM columns (FP32 bit patterns) -> 4 BF16 chunks of the next A operand.
 template <bool RELU>
 __device__ __forceinline__ void store_chunks32(const uint32_t (&v)[32], uint32_t act_row_base, int chunk0) {
 #pragma unroll
@@ -198,15 +202,30 @@ __device__ __forceinline__ void store_chunks32(const uint32_t (&v)[32], uint32_t
   }
 }
 
-// Hash-grid encoding into registers (same arithmetic as the FP32 path).
+// T += V_last[:, j0:j0+32] relu(h[j0:j0+32]) in FP32 (ascending j).
+__device__ __forceinline__ void final_dot32(const uint32_t (&v)[32], const float* __restrict__ sV, int j0,
+                                            float& t0, float& t1, float& t2) {
+#pragma unroll
+  for (int j4 = 0; j4 < 8; ++j4) {
+    const float4 a = *reinterpret_cast<const float4*>(sV + 0 * 64 + j0 + 4 * j4);
+    const float4 b = *reinterpret_cast<const float4*>(sV + 1 * 64 + j0 + 4 * j4);
+    const float4 c = *reinterpret_cast<const float4*>(sV + 2 * 64 + j0 + 4 * j4);
+    const float h0 = fmaxf(__uint_as_float(v[4 * j4 + 0]), 0.f), h1 = fmaxf(__uint_as_float(v[4 * j4 + 1]), 0.f);
+    const float h2 = fmaxf(__uint_as_float(v[4 * j4 + 2]), 0.f), h3 = fmaxf(__uint_as_float(v[4 * j4 + 3]), 0.f);
+    t0 = fmaf(a.x, h0, t0); t0 = fmaf(a.y, h1, t0); t0 = fmaf(a.z, h2, t0); t0 = fmaf(a.w, h3, t0);
+    t1 = fmaf(b.x, h0, t1); t1 = fmaf(b.y, h1, t1); t1 = fmaf(b.z, h2, t1); t1 = fmaf(b.w, h3, t1);
+    t2 = fmaf(c.x, h0, t2); t2 = fmaf(c.y, h1, t2); t2 = fmaf(c.z, h2, t2); t2 = fmaf(c.w, h3, t2);
+  }
+}
+
+// Hash-grid encoding (same arithmetic as the FP32 path), kept as BF16 pairs.
 template <int DMAX>
-__device__ __forceinline__ void hash_encode_regs(const HashLevels& hl, const float* __restrict__ table,
-                                                 float px, float py, float pz, float (&enc)[DMAX]) {
+__device__ __forceinline__ void hash_encode_bf16(const HashLevels& hl, const float* __restrict__ table,
+                                                 float px, float py, float pz, uint32_t (&enc)[DMAX / 2]) {
   const float p[3] = {fminf(fmaxf(px, 0.f), 1.f), fminf(fmaxf(py, 0.f), 1.f), fminf(fmaxf(pz, 0.f), 1.f)};
 #pragma unroll
-  for (int i = 0; i < DMAX; ++i) enc[i] = 0.f;
-#pragma unroll
   for (int l = 0; l < DMAX / 2; ++l) {
+    float a0 = 0.f, a1 = 0.f;
     if (l < hl.n_levels) {
       const int N = hl.res[l];
       uint32_t i0[3];
@@ -223,7 +242,6 @@ __device__ __forceinline__ void hash_encode_regs(const HashLevels& hl, const flo
       const bool dense = (hl.dense_mask >> l) & 1u;
       const uint32_t T = hl.size[l];
       const float2* lvl = reinterpret_cast<const float2*>(table) + hl.offset[l];
-      float a0 = 0.f, a1 = 0.f;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         const uint32_t bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
@@ -238,26 +256,26 @@ __device__ __forceinline__ void hash_encode_regs(const HashLevels& hl, const flo
         a0 = fmaf(wc, v.x, a0);
         a1 = fmaf(wc, v.y, a1);
       }
-      enc[2 * l] = a0;
-      enc[2 * l + 1] = a1;
     }
+    enc[l] = pack_bf16(a0, a1);
   }
 }
 
 // First-layer operand of wavelet k: row = hash(p) * E_k, rounded once to BF16.
 template <int DMAX>
-__device__ __forceinline__ void store_cp(const float (&enc)[DMAX], const float* __restrict__ ek, int D,
+__device__ __forceinline__ void store_cp(const uint32_t (&enc)[DMAX / 2], const float* __restrict__ ek, int D,
                                          uint32_t act_row_base) {
 #pragma unroll
   for (int c = 0; c < DMAX / 8; ++c) {
     if (c * 8 < D) {
       const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
       const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
+      const uint32_t h0 = enc[c * 4 + 0], h1 = enc[c * 4 + 1], h2 = enc[c * 4 + 2], h3 = enc[c * 4 + 3];
       st_shared_v4(act_row_base + (uint32_t)c * 128u,
-                   pack_bf16(__fmul_rn(enc[c * 8 + 0], e0.x), __fmul_rn(enc[c * 8 + 1], e0.y)),
-                   pack_bf16(__fmul_rn(enc[c * 8 + 2], e0.z), __fmul_rn(enc[c * 8 + 3], e0.w)),
-                   pack_bf16(__fmul_rn(enc[c * 8 + 4], e1.x), __fmul_rn(enc[c * 8 + 5], e1.y)),
-                   pack_bf16(__fmul_rn(enc[c * 8 + 6], e1.z), __fmul_rn(enc[c * 8 + 7], e1.w)));
+                   pack_bf16(__fmul_rn(bf16_lo(h0), e0.x), __fmul_rn(bf16_hi(h0), e0.y)),
+                   pack_bf16(__fmul_rn(bf16_lo(h1), e0.z), __fmul_rn(bf16_hi(h1), e0.w)),
+                   pack_bf16(__fmul_rn(bf16_lo(h2), e1.x), __fmul_rn(bf16_hi(h2), e1.y)),
+                   pack_bf16(__fmul_rn(bf16_lo(h3), e1.z), __fmul_rn(bf16_hi(h3), e1.w)));
     }
   }
 }
@@ -273,31 +291,56 @@ __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long
 }
 
 struct __align__(8) TcBarriers {
-  uint64_t acc_full[kNWG];   // MMA -> epilogue: accumulator of the current layer ready
-  uint64_t act_ready[kNWG];  // epilogue -> MMA: next A operand written, TMEM drained (4 arrivals)
-  uint64_t done;             // final commit before TMEM is released
+  uint64_t acc_full[kSlots];  // MMA commit -> epilogue of that tile slot
+  uint64_t done[kNWG];        // final commit before TMEM is released
   uint32_t tmem_base;
 };
+
+// Per-slot (tile in flight) state, identical in every thread of the warpgroup.
+struct Slot {
+  long long tile;
+  int job, K, k, l;
+  uint32_t ph;
+  bool live;
+};
+
+__device__ __forceinline__ void issue_layer(const TcParams& p, const TcLayer& L, uint32_t wbase, uint32_t a_base,
+                                            uint32_t aux_base, uint32_t d_tmem, uint64_t* bar) {
+  tc_fence_after();
+  const uint32_t id = idesc_bf16(L.n);
+  for (int s = 0; s < L.k / 16; ++s) {
+    const uint64_t ad = smem_desc(a_base + (uint32_t)s * 256u, 128u, 1024u);
+    const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
+    mma_bf16(d_tmem, ad, bd, id, s > 0 ? 1u : 0u);
+  }
+  if (L.aux) {
+    const uint64_t ad = smem_desc(aux_base, 128u, 256u);
+    const uint64_t bd = smem_desc(wbase + L.aux_off, 128u, 256u);
+    mma_bf16(d_tmem, ad, bd, id, 1u);
+  }
+  mma_commit(bar);
+}
 
 template <int DMAX>
 __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_constant__ TcParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* wsm = smem;                                            // weight blob
-  uint8_t* act = smem + ((p.wblob_bytes + 1023u) & ~1023u);       // [kNWG][kActBytes]
-  uint8_t* aux = act + kNWG * kActBytes;                          // [kNWG][kAuxBytes]
-  TcBarriers* bars = reinterpret_cast<TcBarriers*>(aux + kNWG * kAuxBytes);
+  uint8_t* wsm = smem;                                       // weight blob (+ V_last)
+  uint8_t* act = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kSlots][kActBytes]
+  uint8_t* aux = act + kSlots * kActBytes;                   // [kSlots][kAuxBytes]
+  TcBarriers* bars = reinterpret_cast<TcBarriers*>(aux + kSlots * kAuxBytes);
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
+  const int g = warp >> 2;  // warpgroup
+  const int q = warp & 3;   // TMEM lane quarter this warp may read
+  const int row = q * 32 + lane;
+  const bool leader = (tid & 127) == 0;
 
   // ---- weights -> shared memory (generic proxy), barriers, TMEM
   for (uint32_t i = tid; i < p.wblob_bytes / 16u; i += kThreads)
     reinterpret_cast<uint4*>(wsm)[i] = __ldg(p.wblob + i);
   if (tid == 0) {
-    for (int g = 0; g < kNWG; ++g) {
-      mbar_init(&bars->acc_full[g], 1);
-      mbar_init(&bars->act_ready[g], 4);
-    }
-    mbar_init(&bars->done, 1);
+    for (int s = 0; s < kSlots; ++s) mbar_init(&bars->acc_full[s], 1);
+    for (int w = 0; w < kNWG; ++w) mbar_init(&bars->done[w], 1);
     fence_barrier_init();
   }
   if (warp == 0) {
@@ -312,173 +355,155 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = bars->tmem_base;
+  const uint32_t wbase = smem_u32(wsm);
+  const float* sV = reinterpret_cast<const float*>(wsm + p.vlast_off);
   const long long stride = (long long)gridDim.x * kNWG;
 
-  if (warp == 0) {
-    // ================================================================ MMA issuer
-    if (lane == 0) {
-      const uint32_t wbase = smem_u32(wsm);
-      long long tile[kNWG];
-      int K[kNWG], k[kNWG], l[kNWG];
-      uint32_t ph[kNWG];
-      int live = 0;
-      for (int g = 0; g < kNWG; ++g) {
-        tile[g] = (long long)blockIdx.x * kNWG + g;
-        k[g] = 0;
-        l[g] = 0;
-        ph[g] = 0;
-        K[g] = 0;
-        if (tile[g] < p.total_tiles) {
-          K[g] = p.jobs[find_job(p.jobs, p.n_jobs, tile[g])].K;
-          ++live;
-        }
-      }
-      uint64_t idle_since = 0;
-      bool failed = false;
-      while (live > 0 && !failed) {
-        bool progressed = false;
-        for (int g = 0; g < kNWG; ++g) {
-          if (tile[g] >= p.total_tiles) continue;
-          if (!mbar_test(smem_u32(&bars->act_ready[g]), ph[g])) continue;
-          ph[g] ^= 1u;
-          progressed = true;
-          tc_fence_after();
-          const TcLayer& L = p.layers[l[g]];
-          const uint32_t a_base = smem_u32(act + g * kActBytes);
-          const uint32_t d = tmem + (uint32_t)(g * 64);
-          const uint32_t id = idesc_bf16(L.n);
-          for (int s = 0; s < L.k / 16; ++s) {
-            const uint64_t ad = smem_desc(a_base + (uint32_t)s * 256u, 128u, 1024u);
-            const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
-            mma_bf16(d, ad, bd, id, s > 0 ? 1u : 0u);
-          }
-          if (L.aux) {
-            const uint64_t ad = smem_desc(smem_u32(aux + g * kAuxBytes), 128u, 256u);
-            const uint64_t bd = smem_desc(wbase + L.aux_off, 128u, 256u);
-            mma_bf16(d, ad, bd, id, 1u);
-          }
-          mma_commit(&bars->acc_full[g]);
-          if (++l[g] == p.n_layers) {
-            l[g] = 0;
-            if (++k[g] == K[g]) {
-              k[g] = 0;
-              tile[g] += stride;
-              if (tile[g] < p.total_tiles) K[g] = p.jobs[find_job(p.jobs, p.n_jobs, tile[g])].K;
-              else --live;
-            }
-          }
-        }
-        if (progressed) {
-          idle_since = 0;
-        } else {
-          const uint64_t now = globaltimer();
-          if (idle_since == 0) idle_since = now;
-          else if (now - idle_since > kWaitNs) {
-            atomicCAS(p.err, 0u, (uint32_t)kDevWaitTimeout);
-            failed = true;
-          }
-        }
-      }
-      // every issued MMA has completed before TMEM is released
-      mma_commit(&bars->done);
-      wait_bounded(&bars->done, 0, p.err);
-    }
-  } else {
-    // ================================================================ epilogue warpgroups
-    const int g = (warp - 1) >> 2;
-    const int q = warp & 3;                       // TMEM lane quarter this warp may read
-    const int row = q * 32 + lane;                // tile row = pixel within the tile
-    const uint32_t act_row = smem_u32(act + g * kActBytes) + core_off(row, 0, 1024u);
-    const uint32_t aux_row = smem_u32(aux + g * kAuxBytes) + core_off(row, 0, 256u);
-    const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * 64);
-    uint32_t acc_ph = 0;
-    bool ok = true;
-    for (long long t = (long long)blockIdx.x * kNWG + g; t < p.total_tiles && ok; t += stride) {
-      const TcJob& J = p.jobs[find_job(p.jobs, p.n_jobs, t)];
-      const long long px = (t - J.tile_begin) * kTile + row;
-      const bool valid = px < J.n_px;
-      float enc[DMAX];
-      bool active = false;
-      if (valid) {
-        const float4* pr = reinterpret_cast<const float4*>(J.packed) + px * 4;
-        const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3);
-        hash_encode_regs<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, enc);
-        active = J.flag[px] != 0;
-        // aux operand: the 13 remapped G-buffer values followed by ones
-        st_shared_v4(aux_row, pack_bf16(r0.w, r1.x), pack_bf16(r1.y, r1.z), pack_bf16(r1.w, r2.x),
-                     pack_bf16(r2.y, r2.z));
-        st_shared_v4(aux_row + 128u, pack_bf16(r2.w, r3.x), pack_bf16(r3.y, r3.z), pack_bf16(r3.w, 1.f),
-                     pack_bf16(1.f, 1.f));
-      } else {
+  Slot S[kTPW];
+  uint32_t enc[kTPW][DMAX / 2];
+  float acc[kTPW][6];  // Kahan sums and compensations
+  long long next = (long long)blockIdx.x * kNWG + g;
+  bool ok = true;
+
+  // Starts the next tile of this warpgroup in slot s; returns false when none is left.
+  auto start_tile = [&](int s, Slot& sl, uint32_t (&en)[DMAX / 2], float (&ac)[6]) -> bool {
+    sl.live = false;
+    if (next >= p.total_tiles) return false;
+    sl.tile = next;
+    next += stride;
+    sl.job = find_job(p.jobs, p.n_jobs, sl.tile);
+    const TcJob& J = p.jobs[sl.job];
+    sl.K = J.K;
+    sl.k = 0;
+    sl.l = 0;
+    sl.live = true;
+    const long long px = (sl.tile - J.tile_begin) * kTile + row;
+    const uint32_t act_row = smem_u32(act + (g * kTPW + s) * kActBytes) + core_off(row, 0, 1024u);
+    const uint32_t aux_row = smem_u32(aux + (g * kTPW + s) * kAuxBytes) + core_off(row, 0, 256u);
+    if (px < J.n_px) {
+      const float4* pr = reinterpret_cast<const float4*>(J.packed) + px * 4;
+      const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3);
+      hash_encode_bf16<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, en);
+      // aux operand: the 13 remapped G-buffer values followed by ones
+      st_shared_v4(aux_row, pack_bf16(r0.w, r1.x), pack_bf16(r1.y, r1.z), pack_bf16(r1.w, r2.x),
+                   pack_bf16(r2.y, r2.z));
+      st_shared_v4(aux_row + 128u, pack_bf16(r2.w, r3.x), pack_bf16(r3.y, r3.z), pack_bf16(r3.w, 1.f),
+                   pack_bf16(1.f, 1.f));
+    } else {
 #pragma unroll
-        for (int i = 0; i < DMAX; ++i) enc[i] = 0.f;
-        st_shared_v4(aux_row, 0, 0, 0, 0);
-        st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
-      }
-      store_cp<DMAX>(enc, J.emb_k, p.enc_dims, act_row);
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&bars->act_ready[g]);
-      float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-      for (int k = 0; k < J.K && ok; ++k) {
-        for (int li = 0; li < p.n_layers; ++li) {
-          const TcLayer& L = p.layers[li];
-          // warp-uniform outcome: tcgen05.ld below is .sync.aligned
-          ok = __all_sync(0xffffffffu, wait_bounded(&bars->acc_full[g], acc_ph, p.err));
-          if (!ok) break;
-          acc_ph ^= 1u;
-          tc_fence_after();
-          if (!L.fin) {
-            uint32_t v[32];
-            tmem_ld32(taddr, v);
+      for (int i = 0; i < DMAX / 2; ++i) en[i] = 0u;
+      st_shared_v4(aux_row, 0, 0, 0, 0);
+      st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) ac[i] = 0.f;
+    store_cp<DMAX>(en, J.emb_k, p.enc_dims, act_row);
+    return true;
+  };
+
+  // Makes this thread's shared-memory writes and TMEM reads visible, synchronises the
+  // warpgroup (ANDing the timeout vote) and lets the leader issue slot s's next layer.
+  auto hand_off = [&](int s, Slot& sl) {
+    tc_fence_before();
+    fence_proxy_async_smem();
+    ok = wg_barrier_and(g, ok);
+    if (ok && leader) {
+      const int sid = g * kTPW + s;
+      issue_layer(p, p.layers[sl.l], wbase, smem_u32(act + sid * kActBytes), smem_u32(aux + sid * kAuxBytes),
+                  tmem + (uint32_t)(sid * 64), &bars->acc_full[sid]);
+    }
+  };
+
+#pragma unroll
+  for (int s = 0; s < kTPW; ++s) {
+    S[s].ph = 0;
+    if (start_tile(s, S[s], enc[s], acc[s])) hand_off(s, S[s]);
+  }
+
+  for (;;) {
+    bool any = false;
+#pragma unroll
+    for (int s = 0; s < kTPW; ++s) {
+      Slot& sl = S[s];
+      if (!sl.live || !ok) continue;
+      any = true;
+      const int sid = g * kTPW + s;
+      const uint32_t act_row = smem_u32(act + sid * kActBytes) + core_off(row, 0, 1024u);
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(sid * 64);
+      const bool waited = __all_sync(0xffffffffu, wait_bounded(&bars->acc_full[sid], sl.ph, p.err));
+      sl.ph ^= 1u;
+      const TcLayer& L = p.layers[sl.l];
+      if (waited) {
+        tc_fence_after();
+        uint32_t v[32];
+        if (!L.fin) {
+          tmem_ld32(taddr, v);
+          tmem_wait_ld();
+          if (L.relu) store_chunks32<true>(v, act_row, 0);
+          else store_chunks32<false>(v, act_row, 0);
+          if (L.n > 32) {
+            tmem_ld32(taddr + 32u, v);
             tmem_wait_ld();
-            if (L.relu) store_chunks32<true>(v, act_row, 0);
-            else store_chunks32<false>(v, act_row, 0);
-            if (L.n > 32) {
-              tmem_ld32(taddr + 32u, v);
-              tmem_wait_ld();
-              if (L.relu) store_chunks32<true>(v, act_row, 4);
-              else store_chunks32<false>(v, act_row, 4);
-            }
-          } else {
-            uint32_t v[4];
-            tmem_ld4(taddr, v);
-            tmem_wait_ld();
-            const float* Lk = J.strength + (size_t)k * 3;
-            float t0 = __fmul_rn(__ldg(Lk + 0), __uint_as_float(v[0]));
-            float t1 = __fmul_rn(__ldg(Lk + 1), __uint_as_float(v[1]));
-            float t2 = __fmul_rn(__ldg(Lk + 2), __uint_as_float(v[2]));
-            if (p.clamp) { t0 = fmaxf(t0, 0.f); t1 = fmaxf(t1, 0.f); t2 = fmaxf(t2, 0.f); }
-            if (p.kahan) {
-              float y, z;
-              y = __fsub_rn(t0, c0); z = __fadd_rn(s0, y); c0 = __fsub_rn(__fsub_rn(z, s0), y); s0 = z;
-              y = __fsub_rn(t1, c1); z = __fadd_rn(s1, y); c1 = __fsub_rn(__fsub_rn(z, s1), y); s1 = z;
-              y = __fsub_rn(t2, c2); z = __fadd_rn(s2, y); c2 = __fsub_rn(__fsub_rn(z, s2), y); s2 = z;
-            } else {
-              s0 = __fadd_rn(s0, t0); s1 = __fadd_rn(s1, t1); s2 = __fadd_rn(s2, t2);
-            }
-            if (k + 1 < J.K) store_cp<DMAX>(enc, J.emb_k + (size_t)(k + 1) * p.enc_dims, p.enc_dims, act_row);
+            if (L.relu) store_chunks32<true>(v, act_row, 4);
+            else store_chunks32<false>(v, act_row, 4);
           }
-          const bool last = L.fin && k + 1 == J.K;  // the next tile's set-up arrives instead
-          if (!last) {
-            tc_fence_before();
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars->act_ready[g]);
+        } else {
+          float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+          tmem_ld32(taddr, v);
+          tmem_wait_ld();
+          final_dot32(v, sV, 0, t0, t1, t2);
+          tmem_ld32(taddr + 32u, v);
+          tmem_wait_ld();
+          final_dot32(v, sV, 32, t0, t1, t2);
+          const TcJob& J = p.jobs[sl.job];
+          const float* Lk = J.strength + (size_t)sl.k * 3;
+          float u0 = __fmul_rn(__ldg(Lk + 0), t0);
+          float u1 = __fmul_rn(__ldg(Lk + 1), t1);
+          float u2 = __fmul_rn(__ldg(Lk + 2), t2);
+          if (p.clamp) { u0 = fmaxf(u0, 0.f); u1 = fmaxf(u1, 0.f); u2 = fmaxf(u2, 0.f); }
+          float* a = acc[s];
+          if (p.kahan) {
+            float y, z;
+            y = __fsub_rn(u0, a[3]); z = __fadd_rn(a[0], y); a[3] = __fsub_rn(__fsub_rn(z, a[0]), y); a[0] = z;
+            y = __fsub_rn(u1, a[4]); z = __fadd_rn(a[1], y); a[4] = __fsub_rn(__fsub_rn(z, a[1]), y); a[1] = z;
+            y = __fsub_rn(u2, a[5]); z = __fadd_rn(a[2], y); a[5] = __fsub_rn(__fsub_rn(z, a[2]), y); a[2] = z;
           } else {
+            a[0] = __fadd_rn(a[0], u0); a[1] = __fadd_rn(a[1], u1); a[2] = __fadd_rn(a[2], u2);
+          }
+          if (sl.k + 1 < sl.K) store_cp<DMAX>(enc[s], J.emb_k + (size_t)(sl.k + 1) * p.enc_dims, p.enc_dims, act_row);
+        }
+      }
+      // advance the slot: next layer, next wavelet, or the next tile
+      if (++sl.l == p.n_layers) {
+        sl.l = 0;
+        if (++sl.k == sl.K) {
+          const TcJob& J = p.jobs[sl.job];
+          const long long px = (sl.tile - J.tile_begin) * kTile + row;
+          if (px < J.n_px && waited) {
+            const float* a = acc[s];
+            const float4 ind = J.flag[px] ? make_float4(a[0], a[1], a[2], 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
+            const float4 dl = __ldg(reinterpret_cast<const float4*>(J.direct) + px);
+            reinterpret_cast<float4*>(J.indirect)[px] = ind;
+            reinterpret_cast<float4*>(J.with_direct)[px] =
+                make_float4(__fadd_rn(ind.x, dl.x), __fadd_rn(ind.y, dl.y), __fadd_rn(ind.z, dl.z), 1.f);
+          }
+          if (!start_tile(s, sl, enc[s], acc[s])) {
+            // no further tile for this slot: still vote so the warpgroup stays in step
             tc_fence_before();
+            ok = wg_barrier_and(g, ok && waited);
+            continue;
           }
         }
       }
-      if (valid && ok) {
-        float4 ind = make_float4(0.f, 0.f, 0.f, 1.f);
-        if (active) ind = make_float4(s0, s1, s2, 1.f);
-        const float4 dl = __ldg(reinterpret_cast<const float4*>(J.direct) + px);
-        reinterpret_cast<float4*>(J.indirect)[px] = ind;
-        reinterpret_cast<float4*>(J.with_direct)[px] =
-            make_float4(__fadd_rn(ind.x, dl.x), __fadd_rn(ind.y, dl.y), __fadd_rn(ind.z, dl.z), 1.f);
-      }
+      ok = ok && waited;
+      hand_off(s, sl);
     }
+    if (!any || !ok) break;
+  }
+  // every MMA this warpgroup issued has completed before TMEM is released
+  if (leader) {
+    mma_commit(&bars->done[g]);
+    wait_bounded(&bars->done[g], 0, p.err);
   }
   tc_fence_before();
   __syncthreads();
@@ -518,6 +543,7 @@ void put_b(std::vector<uint16_t>* blob, size_t off, const float* src, int n, int
 struct Plan {
   TcLayer layers[kMaxTcLayers];
   int n_layers = 0;
+  uint32_t vlast_off = 0;
   std::vector<uint16_t> blob;
 };
 
@@ -526,32 +552,30 @@ bool plan_supported(const NetDims& d, std::string* why) {
   if (d.aux_width != 16) return no("tensor-core path needs a 16-wide aux encoding");
   if (d.enc_dims() % 16 || d.enc_dims() > 32) return no("tensor-core path needs 16 or 32 hash features");
   if (d.op_out > 64) return no("tensor-core path needs out_prd outputs <= 64");
-  if (d.op_nl + d.cn_nl > kMaxTcLayers) return no("too many layers for the tensor-core path");
-  for (int i = 0; i < d.op_nl; ++i)
-    if (pad16(d.op_outs[i]) > 64 || (i > 0 && pad16(d.op_in[i]) > 64)) return no("tensor-core path needs widths <= 64");
-  for (int i = 1; i < d.cn_nl; ++i)
-    if (pad16(d.cn_in[i]) > 64 || pad16(d.cn_outs[i]) > 64) return no("tensor-core path needs widths <= 64");
-  if (pad16(d.cn_outs[0]) > 64) return no("tensor-core path needs widths <= 64");
-  for (int i = 0; i < d.op_nl; ++i)
-    if (pad16(d.op_outs[i]) == 48 || pad16(d.op_outs[i]) == 16) return no("hidden widths must pad to 32 or 64");
-  for (int i = 0; i + 1 < d.cn_nl; ++i)
-    if (pad16(d.cn_outs[i]) == 48 || pad16(d.cn_outs[i]) == 16) return no("hidden widths must pad to 32 or 64");
+  if (d.cn_hidden < 1) return no("tensor-core path needs a hidden cmp_net layer");
+  if (d.cn_neurons > 64 || pad16(d.cn_neurons) != 64) return no("tensor-core path needs 64-wide cmp_net layers");
+  if (d.op_nl + d.cn_nl - 1 > kMaxTcLayers) return no("too many layers for the tensor-core path");
+  for (int i = 0; i < d.op_nl; ++i) {
+    const int n = pad16(d.op_outs[i]);
+    if (n != 32 && n != 64) return no("out_prd widths must pad to 32 or 64");
+    if (i > 0 && pad16(d.op_in[i]) > 64) return no("tensor-core path needs widths <= 64");
+  }
   return true;
 }
 
 Plan make_plan(const NetDims& d, const float* op, const float* cn) {
   Plan P;
   size_t off = 0;
-  auto add = [&](const float* W, int n, int k_total, int col0, int kc, bool relu, bool fin) {
+  const bool fill = op && cn;
+  auto add = [&](const float* W, int n, int k_total, int col0, int kc, bool relu) {
     TcLayer L{};
-    const int np = fin ? 16 : pad16(n), kp = pad16(kc);
+    const int np = pad16(n), kp = pad16(kc);
     L.b_off = (uint32_t)off;
     L.b_sbo = (uint32_t)kp * 16u;
     L.k = kp;
     L.n = np;
     L.relu = relu;
-    L.fin = fin;
-    if (op || cn) put_b(&P.blob, off, W, n, k_total, col0, kc, np, kp);
+    if (fill) put_b(&P.blob, off, W, n, k_total, col0, kc, np, kp);
     off += (size_t)np * kp * 2;
     off = (off + 127) & ~size_t(127);
     P.layers[P.n_layers++] = L;
@@ -559,26 +583,41 @@ Plan make_plan(const NetDims& d, const float* op, const float* cn) {
   };
   const float* w = op;
   for (int i = 0; i < d.op_nl; ++i) {
-    add(w, d.op_outs[i], d.op_in[i], 0, d.op_in[i], i + 1 < d.op_nl, false);
+    add(w, d.op_outs[i], d.op_in[i], 0, d.op_in[i], i + 1 < d.op_nl);
     if (w) w += (size_t)d.op_in[i] * d.op_outs[i];
   }
   w = cn;
-  for (int i = 0; i < d.cn_nl; ++i) {
-    const bool fin = i + 1 == d.cn_nl;
+  for (int i = 0; i + 1 < d.cn_nl; ++i) {
+    int li;
     if (i == 0) {
-      const int li = add(w, d.cn_outs[0], d.cn_in[0], 0, d.op_out, !fin, fin);
+      li = add(w, d.cn_outs[0], d.cn_in[0], 0, d.op_out, true);
       // aux block: columns [op_out, op_out + 16) of cmp_net's first layer
       P.layers[li].aux = 1;
       P.layers[li].aux_off = (uint32_t)off;
-      const int np = fin ? 16 : pad16(d.cn_outs[0]);
-      if (op || cn) put_b(&P.blob, off, w, d.cn_outs[0], d.cn_in[0], d.op_out, 16, np, 16);
+      const int np = pad16(d.cn_outs[0]);
+      if (fill) put_b(&P.blob, off, w, d.cn_outs[0], d.cn_in[0], d.op_out, 16, np, 16);
       off += (size_t)np * 16 * 2;
       off = (off + 127) & ~size_t(127);
     } else {
-      add(w, d.cn_outs[i], d.cn_in[i], 0, d.cn_in[i], !fin, fin);
+      li = add(w, d.cn_outs[i], d.cn_in[i], 0, d.cn_in[i], true);
     }
     if (w) w += (size_t)d.cn_in[i] * d.cn_outs[i];
   }
+  P.layers[P.n_layers - 1].fin = 1;
+  // V_last: the 3 x 64 output layer in FP32, [c][j]
+  P.vlast_off = (uint32_t)off;
+  const size_t vbytes = kVlastFloats * 4;
+  P.blob.resize((off + vbytes) / 2, 0);
+  if (fill) {
+    const int n_in = d.cn_in[d.cn_nl - 1];
+    for (int c = 0; c < 3; ++c)
+      for (int j = 0; j < 64; ++j) {
+        const float v = j < n_in ? w[(size_t)c * n_in + j] : 0.f;
+        std::memcpy(reinterpret_cast<char*>(P.blob.data()) + off + (c * 64 + j) * 4, &v, 4);
+      }
+  }
+  off += vbytes;
+  off = (off + 127) & ~size_t(127);
   P.blob.resize(off / 2, 0);
   return P;
 }
@@ -594,7 +633,7 @@ void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::ve
 }
 
 size_t relight_tc_smem_bytes(const NetDims& d) {
-  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * (kActBytes + kAuxBytes) +
+  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kSlots * (kActBytes + kAuxBytes) +
          sizeof(TcBarriers);
 }
 
@@ -610,6 +649,7 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.hash = hash;
   p.wblob = reinterpret_cast<const uint4*>(tc_weights_dev);
   p.wblob_bytes = (uint32_t)(P.blob.size() * 2);
+  p.vlast_off = P.vlast_off;
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
   p.n_layers = P.n_layers;
   p.enc_dims = d.enc_dims();
