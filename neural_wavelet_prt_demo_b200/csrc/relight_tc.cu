@@ -3,26 +3,29 @@
 // Same computation as the FP32 path (prt_network.h:73-154 + utils_kernels.h:52-127):
 // per pixel p and wavelet k, cp = hash(p) * E[:, idx_k] -> out_prd MLP -> [o || aux]
 // -> cmp_net MLP -> T_k, and sum_k max(L_k * T_k, 0).  Every hidden dense layer of a
-// 128-pixel x 1-wavelet row block is issued as tcgen05.mma (M=128, N<=64, K=16 steps);
+// 128-pixel x 1-wavelet row block is one tcgen05.mma chain (M=128, N<=64, K=16 steps);
 // the final 3-output layer runs in FP32 on the CUDA cores inside the epilogue of the
 // layer before it, straight from the FP32 accumulator.
 //
-// Measured on B200: a tcgen05.mma costs >= ~60 cycles whatever N <= 64 (N=128 takes 64,
-// N=256 128), so these 64-wide layers are issue-bound at ~53% of the tensor peak; the
-// kernel's job is to keep that issue slot busy.  Organisation (one persistent CTA per SM):
-//   kNWG warpgroups x kTPW tiles: warpgroup g keeps kTPW 128-pixel tiles in flight, each
-//   with its own 64 TMEM columns and its own A-operand buffers in shared memory.  While
-//   the tensor core runs one tile's layer the warpgroup drains another tile's accumulator.
-//   Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may read.
-// Per layer of a tile: wait acc barrier -> tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 ->
-// st.shared into the next A operand (canonical K-major, no swizzle: 8x16B core matrices,
-// LBO = 128 B between K chunks, SBO = 1024 B between 8-row groups) -> fence.proxy.async
-// -> warpgroup barrier (bar.red.and carrying the "no timeout" vote) -> one elected thread
-// issues the next layer's MMAs and commits them to the tile's barrier.
-// The final layer's epilogue forms T_k = V_last relu(h) in FP32, does the clamped Kahan
-// sum and writes the next wavelet's first-layer operand hash(p) * E_k+1, so the
-// transport never leaves the SM.  Every wait is bounded by %globaltimer (2 s); on expiry
-// the kernel records kDevWaitTimeout and the whole warpgroup unwinds together.
+// Design, from measurements on B200: a tcgen05.mma costs >= ~60 cycles whatever N <= 64,
+// so these 64-wide layers are bound by MMA issue at ~53% of the tensor peak; keeping the
+// activations in shared memory made the kernel shared-memory-bandwidth bound instead
+// (operand reads + epilogue stores ~266 KB per tile and wavelet).  So activations live
+// in TMEM: the A operand of every layer is read by the MMA straight from tensor memory
+// (the ".kind::f16 [d], [a], b_desc" form), and the epilogue writes it back with a
+// single tcgen05.st.  Only the weights (B) and the per-tile aux block come from shared
+// memory.
+//
+// Organisation (one persistent CTA per SM): kNWG warpgroups, one 128-pixel tile each,
+// 128 TMEM columns per tile: [0,32) the BF16 A operand (2 values per 32-bit column),
+// [64,128) the FP32 accumulator.  Thread (warp w, lane l) owns tile row 32*(w%4)+l, the
+// TMEM lane it may access.  Per layer: wait on the tile's commit barrier -> tcgen05.ld
+// -> ReLU + cvt.rn.relu.bf16x2 -> tcgen05.st into the A columns -> warpgroup barrier
+// (bar.red.and carrying the "no timeout" vote) -> one elected thread issues the next
+// layer's MMAs and commits them.  The final layer's epilogue forms T_k, does the
+// clamped Kahan sum and writes the next wavelet's first-layer operand hash(p) * E_k+1.
+// Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
+// kDevWaitTimeout and the warpgroup unwinds together.
 #include <cmath>
 #include <cstring>
 
@@ -31,18 +34,18 @@
 namespace nwprt {
 namespace {
 
-constexpr int kNWG = 4;                    // warpgroups per CTA
-constexpr int kTPW = 2;                    // tiles in flight per warpgroup
+constexpr int kNWG = 4;                    // warpgroups per CTA, one tile each
 constexpr int kThreads = 128 * kNWG;
-constexpr int kSlots = kNWG * kTPW;
 constexpr int kTile = 128;                 // pixels per tile (MMA M)
-constexpr int kActBytes = kTile * 64 * 2;  // 128 x 64 bf16
-constexpr int kAuxBytes = kTile * 16 * 2;  // 128 x 16 bf16
+constexpr int kAuxBytes = kTile * 16 * 2;  // 128 x 16 bf16 aux operand
 constexpr int kMaxTcLayers = 12;
 constexpr int kTmemCols = 512;
+constexpr int kTileCols = 128;             // TMEM columns per tile
+constexpr int kAcol = 0;                   // A operand columns [0, 32)
+constexpr int kDcol = 64;                  // accumulator columns [64, 128)
 constexpr int kVlastFloats = 3 * 64;
 constexpr uint64_t kWaitNs = 2000000000ull;
-static_assert(kSlots * 64 <= kTmemCols, "TMEM budget");
+static_assert(kNWG * kTileCols <= kTmemCols, "TMEM budget");
 
 struct TcLayer {
   uint32_t b_off;  // byte offset of B (N x K, canonical K-major) in the weight blob
@@ -127,8 +130,20 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
-                                         uint32_t accumulate) {
+// D[tmem] (+)= A[tmem] * B[smem]^T
+__device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T
+__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
@@ -150,9 +165,12 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 #define NWPRT_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
                     "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
+#define NWPRT_W8(i) "r"(r[i]), "r"(r[i + 1]), "r"(r[i + 2]), "r"(r[i + 3]), "r"(r[i + 4]), \
+                    "r"(r[i + 5]), "r"(r[i + 6]), "r"(r[i + 7])
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -161,6 +179,29 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
       "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
       : NWPRT_R8(0), NWPRT_R8(8), NWPRT_R8(16), NWPRT_R8(24)
       : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      NWPRT_W8(0), NWPRT_W8(8), NWPRT_W8(16), NWPRT_W8(24)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+      NWPRT_W8(0), NWPRT_W8(8)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+               NWPRT_W8(0)
+               : "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -187,18 +228,13 @@ __device__ __forceinline__ uint32_t core_off(int row, int chunk, uint32_t sbo) {
   return (uint32_t)(row >> 3) * sbo + (uint32_t)chunk * 128u + (uint32_t)(row & 7) * 16u;
 }
 
-// 32 TMEM columns (FP32 bit patterns) -> 4 BF16 chunks of the next A operand.
+// 32 FP32 TMEM values -> 16 BF16 pairs.
 template <bool RELU>
-__device__ __forceinline__ void store_chunks32(const uint32_t (&v)[32], uint32_t act_row_base, int chunk0) {
+__device__ __forceinline__ void pack32(const uint32_t (&v)[32], uint32_t* out) {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    uint32_t q[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float lo = __uint_as_float(v[c * 8 + 2 * j]), hi = __uint_as_float(v[c * 8 + 2 * j + 1]);
-      q[j] = RELU ? pack_bf16_relu(lo, hi) : pack_bf16(lo, hi);
-    }
-    st_shared_v4(act_row_base + (uint32_t)(chunk0 + c) * 128u, q[0], q[1], q[2], q[3]);
+  for (int j = 0; j < 16; ++j) {
+    const float lo = __uint_as_float(v[2 * j]), hi = __uint_as_float(v[2 * j + 1]);
+    out[j] = RELU ? pack_bf16_relu(lo, hi) : pack_bf16(lo, hi);
   }
 }
 
@@ -261,23 +297,23 @@ __device__ __forceinline__ void hash_encode_bf16(const HashLevels& hl, const flo
   }
 }
 
-// First-layer operand of wavelet k: row = hash(p) * E_k, rounded once to BF16.
+// First-layer operand of wavelet k (hash(p) * E_k, rounded once to BF16) -> TMEM A columns.
 template <int DMAX>
-__device__ __forceinline__ void store_cp(const uint32_t (&enc)[DMAX / 2], const float* __restrict__ ek, int D,
-                                         uint32_t act_row_base) {
+__device__ __forceinline__ void store_cp(const uint32_t (&enc)[DMAX / 2], const float* __restrict__ ek,
+                                         uint32_t a_taddr) {
+  uint32_t cp[DMAX / 2];
 #pragma unroll
   for (int c = 0; c < DMAX / 8; ++c) {
-    if (c * 8 < D) {
-      const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
-      const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
-      const uint32_t h0 = enc[c * 4 + 0], h1 = enc[c * 4 + 1], h2 = enc[c * 4 + 2], h3 = enc[c * 4 + 3];
-      st_shared_v4(act_row_base + (uint32_t)c * 128u,
-                   pack_bf16(__fmul_rn(bf16_lo(h0), e0.x), __fmul_rn(bf16_hi(h0), e0.y)),
-                   pack_bf16(__fmul_rn(bf16_lo(h1), e0.z), __fmul_rn(bf16_hi(h1), e0.w)),
-                   pack_bf16(__fmul_rn(bf16_lo(h2), e1.x), __fmul_rn(bf16_hi(h2), e1.y)),
-                   pack_bf16(__fmul_rn(bf16_lo(h3), e1.z), __fmul_rn(bf16_hi(h3), e1.w)));
-    }
+    const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
+    const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
+    const uint32_t h0 = enc[c * 4 + 0], h1 = enc[c * 4 + 1], h2 = enc[c * 4 + 2], h3 = enc[c * 4 + 3];
+    cp[c * 4 + 0] = pack_bf16(__fmul_rn(bf16_lo(h0), e0.x), __fmul_rn(bf16_hi(h0), e0.y));
+    cp[c * 4 + 1] = pack_bf16(__fmul_rn(bf16_lo(h1), e0.z), __fmul_rn(bf16_hi(h1), e0.w));
+    cp[c * 4 + 2] = pack_bf16(__fmul_rn(bf16_lo(h2), e1.x), __fmul_rn(bf16_hi(h2), e1.y));
+    cp[c * 4 + 3] = pack_bf16(__fmul_rn(bf16_lo(h3), e1.z), __fmul_rn(bf16_hi(h3), e1.w));
   }
+  if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
+  else tmem_st8(a_taddr, cp);
 }
 
 __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long tile) {
@@ -291,32 +327,24 @@ __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long
 }
 
 struct __align__(8) TcBarriers {
-  uint64_t acc_full[kSlots];  // MMA commit -> epilogue of that tile slot
-  uint64_t done[kNWG];        // final commit before TMEM is released
+  uint64_t acc_full[kNWG];  // MMA commit -> epilogue of that warpgroup's tile
+  uint64_t done[kNWG];      // final commit before TMEM is released
   uint32_t tmem_base;
 };
 
-// Per-slot (tile in flight) state, identical in every thread of the warpgroup.
-struct Slot {
-  long long tile;
-  int job, K, k, l;
-  uint32_t ph;
-  bool live;
-};
-
-__device__ __forceinline__ void issue_layer(const TcParams& p, const TcLayer& L, uint32_t wbase, uint32_t a_base,
-                                            uint32_t aux_base, uint32_t d_tmem, uint64_t* bar) {
+// Issues layer L of warpgroup g's tile: A from TMEM (and the aux block from shared memory).
+__device__ __forceinline__ void issue_layer(const TcLayer& L, uint32_t wbase, uint32_t a_tmem, uint32_t aux_base,
+                                            uint32_t d_tmem, uint64_t* bar) {
   tc_fence_after();
   const uint32_t id = idesc_bf16(L.n);
   for (int s = 0; s < L.k / 16; ++s) {
-    const uint64_t ad = smem_desc(a_base + (uint32_t)s * 256u, 128u, 1024u);
     const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
-    mma_bf16(d_tmem, ad, bd, id, s > 0 ? 1u : 0u);
+    mma_ts(d_tmem, a_tmem + (uint32_t)s * 8u, bd, id, s > 0 ? 1u : 0u);
   }
   if (L.aux) {
     const uint64_t ad = smem_desc(aux_base, 128u, 256u);
     const uint64_t bd = smem_desc(wbase + L.aux_off, 128u, 256u);
-    mma_bf16(d_tmem, ad, bd, id, 1u);
+    mma_ss(d_tmem, ad, bd, id, 1u);
   }
   mma_commit(bar);
 }
@@ -325,13 +353,12 @@ template <int DMAX>
 __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_constant__ TcParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;                                       // weight blob (+ V_last)
-  uint8_t* act = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kSlots][kActBytes]
-  uint8_t* aux = act + kSlots * kActBytes;                   // [kSlots][kAuxBytes]
-  TcBarriers* bars = reinterpret_cast<TcBarriers*>(aux + kSlots * kAuxBytes);
+  uint8_t* aux = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kNWG][kAuxBytes]
+  TcBarriers* bars = reinterpret_cast<TcBarriers*>(aux + kNWG * kAuxBytes);
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int g = warp >> 2;  // warpgroup
-  const int q = warp & 3;   // TMEM lane quarter this warp may read
+  const int q = warp & 3;   // TMEM lane quarter this warp may access
   const int row = q * 32 + lane;
   const bool leader = (tid & 127) == 0;
 
@@ -339,8 +366,10 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   for (uint32_t i = tid; i < p.wblob_bytes / 16u; i += kThreads)
     reinterpret_cast<uint4*>(wsm)[i] = __ldg(p.wblob + i);
   if (tid == 0) {
-    for (int s = 0; s < kSlots; ++s) mbar_init(&bars->acc_full[s], 1);
-    for (int w = 0; w < kNWG; ++w) mbar_init(&bars->done[w], 1);
+    for (int w = 0; w < kNWG; ++w) {
+      mbar_init(&bars->acc_full[w], 1);
+      mbar_init(&bars->done[w], 1);
+    }
     fence_barrier_init();
   }
   if (warp == 0) {
@@ -358,32 +387,29 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   const uint32_t wbase = smem_u32(wsm);
   const float* sV = reinterpret_cast<const float*>(wsm + p.vlast_off);
   const long long stride = (long long)gridDim.x * kNWG;
+  const uint32_t col0 = tmem + (uint32_t)(g * kTileCols);
+  const uint32_t a_tmem = col0 + kAcol;                                 // MMA operand address (lane 0)
+  const uint32_t d_tmem = col0 + kDcol;
+  const uint32_t a_taddr = a_tmem + ((uint32_t)(q * 32) << 16);         // this warp's lanes
+  const uint32_t d_taddr = d_tmem + ((uint32_t)(q * 32) << 16);
+  const uint32_t aux_base = smem_u32(aux + g * kAuxBytes);
+  const uint32_t aux_row = aux_base + core_off(row, 0, 256u);
+  uint64_t* acc_bar = &bars->acc_full[g];
 
-  Slot S[kTPW];
-  uint32_t enc[kTPW][DMAX / 2];
-  float acc[kTPW][6];  // Kahan sums and compensations
-  long long next = (long long)blockIdx.x * kNWG + g;
+  uint32_t ph = 0;
   bool ok = true;
-
-  // Starts the next tile of this warpgroup in slot s; returns false when none is left.
-  auto start_tile = [&](int s, Slot& sl, uint32_t (&en)[DMAX / 2], float (&ac)[6]) -> bool {
-    sl.live = false;
-    if (next >= p.total_tiles) return false;
-    sl.tile = next;
-    next += stride;
-    sl.job = find_job(p.jobs, p.n_jobs, sl.tile);
-    const TcJob& J = p.jobs[sl.job];
-    sl.K = J.K;
-    sl.k = 0;
-    sl.l = 0;
-    sl.live = true;
-    const long long px = (sl.tile - J.tile_begin) * kTile + row;
-    const uint32_t act_row = smem_u32(act + (g * kTPW + s) * kActBytes) + core_off(row, 0, 1024u);
-    const uint32_t aux_row = smem_u32(aux + (g * kTPW + s) * kAuxBytes) + core_off(row, 0, 256u);
-    if (px < J.n_px) {
+  for (long long t = (long long)blockIdx.x * kNWG + g; t < p.total_tiles && ok; t += stride) {
+    // ---- tile set-up: hash encoding, aux operand, first-layer operand of wavelet 0
+    const int jid = find_job(p.jobs, p.n_jobs, t);
+    const TcJob& J = p.jobs[jid];
+    const int K = J.K;
+    const long long px = (t - J.tile_begin) * kTile + row;
+    const bool valid = px < J.n_px;
+    uint32_t enc[DMAX / 2];
+    if (valid) {
       const float4* pr = reinterpret_cast<const float4*>(J.packed) + px * 4;
       const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3);
-      hash_encode_bf16<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, en);
+      hash_encode_bf16<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, enc);
       // aux operand: the 13 remapped G-buffer values followed by ones
       st_shared_v4(aux_row, pack_bf16(r0.w, r1.x), pack_bf16(r1.y, r1.z), pack_bf16(r1.w, r2.x),
                    pack_bf16(r2.y, r2.z));
@@ -391,114 +417,87 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
                    pack_bf16(1.f, 1.f));
     } else {
 #pragma unroll
-      for (int i = 0; i < DMAX / 2; ++i) en[i] = 0u;
+      for (int i = 0; i < DMAX / 2; ++i) enc[i] = 0u;
       st_shared_v4(aux_row, 0, 0, 0, 0);
       st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
     }
-#pragma unroll
-    for (int i = 0; i < 6; ++i) ac[i] = 0.f;
-    store_cp<DMAX>(en, J.emb_k, p.enc_dims, act_row);
-    return true;
-  };
-
-  // Makes this thread's shared-memory writes and TMEM reads visible, synchronises the
-  // warpgroup (ANDing the timeout vote) and lets the leader issue slot s's next layer.
-  auto hand_off = [&](int s, Slot& sl) {
+    store_cp<DMAX>(enc, J.emb_k, a_taddr);
+    tmem_wait_st();
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    // hand the first layer to the tensor core
     tc_fence_before();
     fence_proxy_async_smem();
     ok = wg_barrier_and(g, ok);
-    if (ok && leader) {
-      const int sid = g * kTPW + s;
-      issue_layer(p, p.layers[sl.l], wbase, smem_u32(act + sid * kActBytes), smem_u32(aux + sid * kAuxBytes),
-                  tmem + (uint32_t)(sid * 64), &bars->acc_full[sid]);
-    }
-  };
-
-#pragma unroll
-  for (int s = 0; s < kTPW; ++s) {
-    S[s].ph = 0;
-    if (start_tile(s, S[s], enc[s], acc[s])) hand_off(s, S[s]);
-  }
-
-  for (;;) {
-    bool any = false;
-#pragma unroll
-    for (int s = 0; s < kTPW; ++s) {
-      Slot& sl = S[s];
-      if (!sl.live || !ok) continue;
-      any = true;
-      const int sid = g * kTPW + s;
-      const uint32_t act_row = smem_u32(act + sid * kActBytes) + core_off(row, 0, 1024u);
-      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(sid * 64);
-      const bool waited = __all_sync(0xffffffffu, wait_bounded(&bars->acc_full[sid], sl.ph, p.err));
-      sl.ph ^= 1u;
-      const TcLayer& L = p.layers[sl.l];
-      if (waited) {
-        tc_fence_after();
-        uint32_t v[32];
-        if (!L.fin) {
-          tmem_ld32(taddr, v);
-          tmem_wait_ld();
-          if (L.relu) store_chunks32<true>(v, act_row, 0);
-          else store_chunks32<false>(v, act_row, 0);
-          if (L.n > 32) {
-            tmem_ld32(taddr + 32u, v);
+    if (ok && leader) issue_layer(p.layers[0], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+    for (int k = 0; k < K && ok; ++k) {
+      for (int l = 0; l < p.n_layers; ++l) {
+        const TcLayer& L = p.layers[l];
+        const bool waited = __all_sync(0xffffffffu, wait_bounded(acc_bar, ph, p.err));
+        ph ^= 1u;
+        if (waited) {
+          tc_fence_after();
+          uint32_t v[32];
+          if (!L.fin) {
+            uint32_t a[32];
+            tmem_ld32(d_taddr, v);
             tmem_wait_ld();
-            if (L.relu) store_chunks32<true>(v, act_row, 4);
-            else store_chunks32<false>(v, act_row, 4);
-          }
-        } else {
-          float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-          tmem_ld32(taddr, v);
-          tmem_wait_ld();
-          final_dot32(v, sV, 0, t0, t1, t2);
-          tmem_ld32(taddr + 32u, v);
-          tmem_wait_ld();
-          final_dot32(v, sV, 32, t0, t1, t2);
-          const TcJob& J = p.jobs[sl.job];
-          const float* Lk = J.strength + (size_t)sl.k * 3;
-          float u0 = __fmul_rn(__ldg(Lk + 0), t0);
-          float u1 = __fmul_rn(__ldg(Lk + 1), t1);
-          float u2 = __fmul_rn(__ldg(Lk + 2), t2);
-          if (p.clamp) { u0 = fmaxf(u0, 0.f); u1 = fmaxf(u1, 0.f); u2 = fmaxf(u2, 0.f); }
-          float* a = acc[s];
-          if (p.kahan) {
-            float y, z;
-            y = __fsub_rn(u0, a[3]); z = __fadd_rn(a[0], y); a[3] = __fsub_rn(__fsub_rn(z, a[0]), y); a[0] = z;
-            y = __fsub_rn(u1, a[4]); z = __fadd_rn(a[1], y); a[4] = __fsub_rn(__fsub_rn(z, a[1]), y); a[1] = z;
-            y = __fsub_rn(u2, a[5]); z = __fadd_rn(a[2], y); a[5] = __fsub_rn(__fsub_rn(z, a[2]), y); a[2] = z;
+            if (L.relu) pack32<true>(v, a);
+            else pack32<false>(v, a);
+            if (L.n > 32) {
+              tmem_ld32(d_taddr + 32u, v);
+              tmem_wait_ld();
+              if (L.relu) pack32<true>(v, a + 16);
+              else pack32<false>(v, a + 16);
+              tmem_st32(a_taddr, a);
+            } else {
+              tmem_st16(a_taddr, a);
+            }
+            tmem_wait_st();
           } else {
-            a[0] = __fadd_rn(a[0], u0); a[1] = __fadd_rn(a[1], u1); a[2] = __fadd_rn(a[2], u2);
+            float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+            tmem_ld32(d_taddr, v);
+            tmem_wait_ld();
+            final_dot32(v, sV, 0, t0, t1, t2);
+            tmem_ld32(d_taddr + 32u, v);
+            tmem_wait_ld();
+            final_dot32(v, sV, 32, t0, t1, t2);
+            const float* Lk = J.strength + (size_t)k * 3;
+            float u0 = __fmul_rn(__ldg(Lk + 0), t0);
+            float u1 = __fmul_rn(__ldg(Lk + 1), t1);
+            float u2 = __fmul_rn(__ldg(Lk + 2), t2);
+            if (p.clamp) { u0 = fmaxf(u0, 0.f); u1 = fmaxf(u1, 0.f); u2 = fmaxf(u2, 0.f); }
+            if (p.kahan) {
+              float y, z;
+              y = __fsub_rn(u0, c0); z = __fadd_rn(s0, y); c0 = __fsub_rn(__fsub_rn(z, s0), y); s0 = z;
+              y = __fsub_rn(u1, c1); z = __fadd_rn(s1, y); c1 = __fsub_rn(__fsub_rn(z, s1), y); s1 = z;
+              y = __fsub_rn(u2, c2); z = __fadd_rn(s2, y); c2 = __fsub_rn(__fsub_rn(z, s2), y); s2 = z;
+            } else {
+              s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
+            }
+            if (k + 1 < K) {
+              store_cp<DMAX>(enc, J.emb_k + (size_t)(k + 1) * p.enc_dims, a_taddr);
+              tmem_wait_st();
+            }
           }
-          if (sl.k + 1 < sl.K) store_cp<DMAX>(enc[s], J.emb_k + (size_t)(sl.k + 1) * p.enc_dims, p.enc_dims, act_row);
         }
+        ok = ok && waited;
+        if (l + 1 == p.n_layers && k + 1 == K) break;  // the tile's last layer: no hand-off
+        const int nl = (l + 1 == p.n_layers) ? 0 : l + 1;
+        tc_fence_before();
+        ok = wg_barrier_and(g, ok);
+        if (!ok) break;
+        if (leader) issue_layer(p.layers[nl], wbase, a_tmem, aux_base, d_tmem, acc_bar);
       }
-      // advance the slot: next layer, next wavelet, or the next tile
-      if (++sl.l == p.n_layers) {
-        sl.l = 0;
-        if (++sl.k == sl.K) {
-          const TcJob& J = p.jobs[sl.job];
-          const long long px = (sl.tile - J.tile_begin) * kTile + row;
-          if (px < J.n_px && waited) {
-            const float* a = acc[s];
-            const float4 ind = J.flag[px] ? make_float4(a[0], a[1], a[2], 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
-            const float4 dl = __ldg(reinterpret_cast<const float4*>(J.direct) + px);
-            reinterpret_cast<float4*>(J.indirect)[px] = ind;
-            reinterpret_cast<float4*>(J.with_direct)[px] =
-                make_float4(__fadd_rn(ind.x, dl.x), __fadd_rn(ind.y, dl.y), __fadd_rn(ind.z, dl.z), 1.f);
-          }
-          if (!start_tile(s, sl, enc[s], acc[s])) {
-            // no further tile for this slot: still vote so the warpgroup stays in step
-            tc_fence_before();
-            ok = wg_barrier_and(g, ok && waited);
-            continue;
-          }
-        }
-      }
-      ok = ok && waited;
-      hand_off(s, sl);
     }
-    if (!any || !ok) break;
+    if (valid && ok) {
+      const float4 ind = J.flag[px] ? make_float4(s0, s1, s2, 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
+      const float4 dl = __ldg(reinterpret_cast<const float4*>(J.direct) + px);
+      reinterpret_cast<float4*>(J.indirect)[px] = ind;
+      reinterpret_cast<float4*>(J.with_direct)[px] =
+          make_float4(__fadd_rn(ind.x, dl.x), __fadd_rn(ind.y, dl.y), __fadd_rn(ind.z, dl.z), 1.f);
+    }
+    // every thread of the warpgroup agrees on the outcome before the next tile
+    ok = wg_barrier_and(g, ok);
   }
   // every MMA this warpgroup issued has completed before TMEM is released
   if (leader) {
@@ -633,8 +632,7 @@ void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::ve
 }
 
 size_t relight_tc_smem_bytes(const NetDims& d) {
-  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kSlots * (kActBytes + kAuxBytes) +
-         sizeof(TcBarriers);
+  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + sizeof(TcBarriers);
 }
 
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const uint16_t* tc_weights_dev,
