@@ -185,6 +185,15 @@ NWPRT_API nwprt_status nwprt_sh_project(const float* faces, int S, float* L, voi
 /* Per-pixel SH dot product out[p] = (|sum_j T[p][j] L[j]|, 1) (float4 per pixel) -- the
  * light-vector product of __closesthit__SHradiance (device_functions/devicePrograms.cu:479-490)
  * for per-pixel transport vectors.  abs_out = 0 drops the abs of :490. */
+/* nwprt_sh_project without a workspace, for callers that cannot allocate device memory
+ * (a frame loop that must never reach cudaMalloc/cudaFree, which can synchronise the device,
+ * or a host that reserves all device memory up front).  No counterpart in the reference.
+ * The partial sums live in a fixed static device array (373,248 bytes, held by every GPU
+ * that loads the library until exit), so S must be <= 128.  The first call on a device
+ * looks up that array's address with the device current; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+NWPRT_API nwprt_status nwprt_sh_project_static(const float* faces, int S, float* L, void* stream);
 NWPRT_API nwprt_status nwprt_sh_dot(const float* T, int64_t n_px, int n_coeffs, const float* L,
                           int abs_out, float* out, void* stream);
 

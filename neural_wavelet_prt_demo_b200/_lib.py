@@ -22,7 +22,7 @@ EXPORTS = (
     "nwprt_get_network_info", "nwprt_load_weights", "nwprt_load_weights_dir", "nwprt_ready",
     "nwprt_env_from_faces", "nwprt_env_from_wavelets", "nwprt_env_get_wavelets", "nwprt_env_release",
     "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_sync", "nwprt_haar_topk",
-    "nwprt_sh_project_workspace_size", "nwprt_sh_project", "nwprt_sh_dot",
+    "nwprt_sh_project_workspace_size", "nwprt_sh_project", "nwprt_sh_project_static", "nwprt_sh_dot",
 )
 
 
@@ -94,6 +94,7 @@ def lib():
         "nwprt_haar_topk": (_st, [_vp, _i, _i, _i, _vp, _vp, _vp]),
         "nwprt_sh_project_workspace_size": (C.c_size_t, [_i]),
         "nwprt_sh_project": (_st, [_vp, _i, _vp, _vp, C.c_size_t, _vp]),
+        "nwprt_sh_project_static": (_st, [_vp, _i, _vp, _vp]),
         "nwprt_sh_dot": (_st, [_vp, C.c_int64, _i, _vp, _i, _vp, _vp]),
     }
     for name, (res, args) in sig.items():

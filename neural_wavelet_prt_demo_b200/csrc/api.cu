@@ -200,6 +200,11 @@ void check_out(const float* p, const char* what) {
 
 }  // namespace
 
+namespace nwprt {
+// Records a message for nwprt_last_error(NULL) from entry points defined in other files.
+void set_thread_error(const std::string& m) { g_last_error = m; }
+}  // namespace nwprt
+
 extern "C" {
 
 int nwprt_abi_version(void) { return NWPRT_ABI_VERSION; }

@@ -76,6 +76,9 @@ struct NetDims {
 
 NetDims parse_config(const std::string& json_text);
 
+// Sets the calling thread's nwprt_last_error(NULL) message (api.cu).
+void set_thread_error(const std::string& m);
+
 // Hash-grid level table passed by value to kernels.
 struct HashLevels {
   int n_levels, n_features;
