@@ -104,6 +104,18 @@ typedef struct {
   float* with_direct; /* float4 per pixel (fbPredictedIndirectWithDirect) */
 } nwprt_request;
 
+/* A relight of the pixel range [px_begin, px_end) of a prepared frame (pixel index
+ * x + width*y).  Lets a scheduler split large requests into chunks and pack chunks of
+ * many requests into one device pass.  px_end <= 0 means "to the end of the frame". */
+typedef struct {
+  int env_id;
+  int frame_id;
+  float* indirect;    /* float4 per pixel of the whole frame; only the range is written */
+  float* with_direct;
+  int64_t px_begin;
+  int64_t px_end;
+} nwprt_range_request;
+
 /* ---------------------------------------------------------------- library */
 NWPRT_API int nwprt_abi_version(void);
 NWPRT_API const char* nwprt_status_string(nwprt_status s);
@@ -145,6 +157,9 @@ NWPRT_API nwprt_status nwprt_env_from_wavelets(nwprt_ctx* ctx, const int32_t* id
  * topWaveletStrength (EnvironmentMap.h:24-25).  `capacity` = entries available. */
 NWPRT_API nwprt_status nwprt_env_get_wavelets(nwprt_ctx* ctx, int env_id, int32_t* idx_host,
                                     float* strength_host, int capacity, int* K);
+/* Frees the env id.  Its device buffers stay with the context and are reused, in stream
+ * order, by a later registration of K or fewer wavelets -- work already queued that still
+ * reads the env must be on the same stream as that later registration. */
 NWPRT_API nwprt_status nwprt_env_release(nwprt_ctx* ctx, int env_id);
 
 /* ---------------------------------------------------------------- frames */
@@ -166,6 +181,10 @@ NWPRT_API nwprt_status nwprt_relight(nwprt_ctx* ctx, int env_id, int frame_id,
 /* Many relights in one device pass (cross-request batching for serving). */
 NWPRT_API nwprt_status nwprt_relight_batch(nwprt_ctx* ctx, const nwprt_request* reqs, int n_reqs,
                                  const nwprt_relight_opts* opts, void* stream);
+/* Pixel-range relights, all in one device pass for NWPRT_PREC_BF16 (one launch per
+ * range for NWPRT_PREC_FP32).  Ranges of one frame/output may not overlap within a call. */
+NWPRT_API nwprt_status nwprt_relight_ranges(nwprt_ctx* ctx, const nwprt_range_request* reqs, int n_reqs,
+                                            const nwprt_relight_opts* opts, void* stream);
 /* Blocks until all work the context issued has finished -- RenderEngine::TCNNSync
  * (tinycudann/tcnn.cu:154-158). */
 NWPRT_API nwprt_status nwprt_sync(nwprt_ctx* ctx);
@@ -176,6 +195,13 @@ NWPRT_API nwprt_status nwprt_sync(nwprt_ctx* ctx);
  * flat index face*S*S + row*S + col ascending. */
 NWPRT_API nwprt_status nwprt_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx,
                              float* strength, void* stream);
+/* Rotated copy of a cubemap: dst(d) = src(R^T d) for every texel direction d, sampled as
+ * the reference samples its env cubemaps (point filtering, wrap addressing;
+ * device_functions/cubeMap.cu:23-113, Renderer/textures.h:64-68).  R: 9 floats, row-major,
+ * host memory.  src and dst are device buffers of [6][S][S][3] floats and must differ.
+ * Feeds rotated env maps to nwprt_env_from_faces (the reference precomputes such
+ * rotations offline, README "EnvmapRotation" sets). */
+NWPRT_API nwprt_status nwprt_env_rotate(const float* src, int S, const float* R, float* dst, void* stream);
 /* SH projection (order 8, 81 coefficients) of a cubemap [6][S][S][3] -> L[81][3]
  * (the env SH the reference loads from sh/<name>.npy, EnvironmentMap.cpp:70-77).
  * `workspace` must hold nwprt_sh_project_workspace_size(S) bytes of device memory. */

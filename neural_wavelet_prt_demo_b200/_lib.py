@@ -21,7 +21,8 @@ EXPORTS = (
     "nwprt_abi_version", "nwprt_status_string", "nwprt_last_error", "nwprt_create", "nwprt_destroy",
     "nwprt_get_network_info", "nwprt_load_weights", "nwprt_load_weights_dir", "nwprt_ready",
     "nwprt_env_from_faces", "nwprt_env_from_wavelets", "nwprt_env_get_wavelets", "nwprt_env_release",
-    "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_sync", "nwprt_haar_topk",
+    "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_relight_ranges", "nwprt_sync",
+    "nwprt_haar_topk", "nwprt_env_rotate",
     "nwprt_sh_project_workspace_size", "nwprt_sh_project", "nwprt_sh_project_static", "nwprt_sh_dot",
 )
 
@@ -61,6 +62,11 @@ class Request(C.Structure):
                 ("with_direct", C.c_void_p)]
 
 
+class RangeRequest(C.Structure):
+    _fields_ = [("env_id", C.c_int), ("frame_id", C.c_int), ("indirect", C.c_void_p),
+                ("with_direct", C.c_void_p), ("px_begin", C.c_int64), ("px_end", C.c_int64)]
+
+
 _LIB = None
 _vp, _i, _st = C.c_void_p, C.c_int, C.c_int
 
@@ -90,7 +96,9 @@ def lib():
         "nwprt_prepare": (_st, [_vp, _i, C.POINTER(GBuffer), _vp]),
         "nwprt_relight": (_st, [_vp, _i, _i, C.POINTER(RelightOpts), _vp, _vp, _vp]),
         "nwprt_relight_batch": (_st, [_vp, C.POINTER(Request), _i, C.POINTER(RelightOpts), _vp]),
+        "nwprt_relight_ranges": (_st, [_vp, C.POINTER(RangeRequest), _i, C.POINTER(RelightOpts), _vp]),
         "nwprt_sync": (_st, [_vp]),
+        "nwprt_env_rotate": (_st, [_vp, _i, _vp, _vp, _vp]),
         "nwprt_haar_topk": (_st, [_vp, _i, _i, _i, _vp, _vp, _vp]),
         "nwprt_sh_project_workspace_size": (C.c_size_t, [_i]),
         "nwprt_sh_project": (_st, [_vp, _i, _vp, _vp, C.c_size_t, _vp]),

@@ -45,11 +45,19 @@ void dev_free(void* p) {
 struct EnvEntry {
   bool live = false;
   int K = 0;
+  int cap = 0;                // wavelets the buffers below can hold (kept across reuse)
   int32_t* idx = nullptr;
   float* strength = nullptr;
   float* emb_k = nullptr;     // [K][D], valid when emb_ready
   bool emb_ready = false;
 };
+
+void free_env_buffers(EnvEntry& e) {
+  dev_free(e.idx);
+  dev_free(e.strength);
+  dev_free(e.emb_k);
+  e = EnvEntry{};
+}
 
 struct Frame {
   bool prepared = false;
@@ -93,11 +101,7 @@ struct nwprt_ctx {
     dev_free(d_err);
     dev_free(d_stage);
     dev_free(d_jobs);
-    for (auto& e : envs) {
-      dev_free(e.idx);
-      dev_free(e.strength);
-      dev_free(e.emb_k);
-    }
+    for (auto& e : envs) free_env_buffers(e);
     for (auto& f : frames) dev_free(f.packed);
   }
 };
@@ -156,33 +160,46 @@ void ensure_emb(nwprt_ctx* ctx, EnvEntry& e, cudaStream_t st) {
   if (e.emb_ready) return;
   need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
   const int D = ctx->dims.enc_dims();
-  if (!e.emb_k) e.emb_k = dev_alloc<float>((size_t)e.K * D);
   launch_gather_embedding(ctx->d_emb, D, ctx->dims.n_coeffs(), e.idx, e.K, e.emb_k, ctx->d_err, st);
   e.emb_ready = true;
 }
 
-int new_env(nwprt_ctx* ctx, int K) {
-  int id = -1;
-  for (size_t i = 0; i < ctx->envs.size(); ++i)
-    if (!ctx->envs[i].live) { id = (int)i; break; }
+// Registers an env slot for K wavelets.  Released slots are reused in stream order: a slot
+// whose buffers hold >= K wavelets is taken without any allocation, so a serving loop that
+// registers and releases env maps per request does not allocate or synchronise.
+int new_env(nwprt_ctx* ctx, int K, int D) {
+  int id = -1, spare = -1;
+  for (size_t i = 0; i < ctx->envs.size(); ++i) {
+    const EnvEntry& e = ctx->envs[i];
+    if (e.live) continue;
+    if (e.cap >= K && (id < 0 || e.cap < ctx->envs[id].cap)) id = (int)i;
+    if (spare < 0) spare = (int)i;
+  }
   if (id < 0) {
-    ctx->envs.emplace_back();
-    id = (int)ctx->envs.size() - 1;
+    if (spare >= 0) {
+      NWPRT_CUDA(cudaDeviceSynchronize());  // buffers too small: replace them
+      free_env_buffers(ctx->envs[spare]);
+      id = spare;
+    } else {
+      ctx->envs.emplace_back();
+      id = (int)ctx->envs.size() - 1;
+    }
+    EnvEntry& e = ctx->envs[id];
+    e.idx = dev_alloc<int32_t>(K);
+    e.strength = dev_alloc<float>((size_t)K * 3);
+    e.emb_k = dev_alloc<float>((size_t)K * D);
+    e.cap = K;
   }
   EnvEntry& e = ctx->envs[id];
-  e = EnvEntry{};
   e.K = K;
-  e.idx = dev_alloc<int32_t>(K);
-  e.strength = dev_alloc<float>((size_t)K * 3);
+  e.emb_ready = false;
   e.live = true;
   return id;
 }
 
 void release_env(EnvEntry& e) {
-  dev_free(e.idx);
-  dev_free(e.strength);
-  dev_free(e.emb_k);
-  e = EnvEntry{};
+  e.live = false;
+  e.emb_ready = false;
 }
 
 nwprt_relight_opts default_opts() {
@@ -368,7 +385,7 @@ nwprt_status nwprt_env_from_faces(nwprt_ctx* ctx, const float* faces, int on_dev
       NWPRT_CUDA(cudaMemcpyAsync(ctx->d_stage, faces, n * 4, cudaMemcpyHostToDevice, st));
       src = ctx->d_stage;
     }
-    const int id = new_env(ctx, K);
+    const int id = new_env(ctx, K, ctx->dims.enc_dims());
     EnvEntry& e = ctx->envs[id];
     try {
       launch_haar_topk(src, 1, S, K, e.idx, e.strength, ctx->d_err, st);
@@ -392,7 +409,7 @@ nwprt_status nwprt_env_from_wavelets(nwprt_ctx* ctx, const int32_t* idx, const f
     if (!on_device)
       for (int k = 0; k < K; ++k)
         need(idx[k] >= 0 && idx[k] < nc, NWPRT_INVALID_ARG, "wavelet index outside [0, 6*S*S)");
-    const int id = new_env(ctx, K);
+    const int id = new_env(ctx, K, ctx->dims.enc_dims());
     EnvEntry& e = ctx->envs[id];
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     NWPRT_CUDA(cudaMemcpyAsync(e.idx, idx, (size_t)K * 4, kind, st));
@@ -422,7 +439,6 @@ nwprt_status nwprt_env_release(nwprt_ctx* ctx, int env_id) {
   return guarded(ctx, [&] {
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null argument");
     EnvEntry& e = env_at(ctx, env_id);
-    NWPRT_CUDA(cudaDeviceSynchronize());
     release_env(e);
   });
 }
@@ -459,19 +475,36 @@ nwprt_status nwprt_prepare(nwprt_ctx* ctx, int frame_id, const nwprt_gbuffer* g,
   });
 }
 
-static void relight_one(nwprt_ctx* ctx, const nwprt_request& r, const nwprt_relight_opts& o,
-                        cudaStream_t st) {
-  need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
-  EnvEntry& e = env_at(ctx, r.env_id);
+// A relight of pixels [px_begin, px_end) of a prepared frame (px_end <= 0: whole frame).
+struct RangeReq {
+  int env_id, frame_id;
+  float* indirect;
+  float* with_direct;
+  int64_t px_begin, px_end;
+};
+
+static int64_t resolve_range(nwprt_ctx* ctx, RangeReq& r) {
   need(r.frame_id >= 0 && r.frame_id < NWPRT_MAX_FRAMES, NWPRT_INVALID_ARG, "frame id out of range");
   Frame& f = ctx->frames[r.frame_id];
   need(f.prepared, NWPRT_NOT_READY, "frame was not prepared (call nwprt_prepare first)");
+  const int64_t n = (int64_t)f.width * f.height;
+  if (r.px_end <= 0) r.px_end = n;
+  need(r.px_begin >= 0 && r.px_begin <= r.px_end && r.px_end <= n, NWPRT_INVALID_ARG,
+       "pixel range outside the frame");
   check_out(r.indirect, "null indirect output");
   check_out(r.with_direct, "null with_direct output");
+  return n;
+}
+
+static void relight_one(nwprt_ctx* ctx, RangeReq r, const nwprt_relight_opts& o, cudaStream_t st) {
+  need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
+  EnvEntry& e = env_at(ctx, r.env_id);
+  resolve_range(ctx, r);
+  Frame& f = ctx->frames[r.frame_id];
   ensure_emb(ctx, e, st);
-  const int64_t n = (int64_t)f.width * f.height;
   if (o.precision == NWPRT_PREC_FP32) {
-    RelightJob j{f.packed, f.flag, f.direct, e.emb_k, e.strength, e.K, n, r.indirect, r.with_direct};
+    RelightJob j{f.packed, f.flag, f.direct, e.emb_k, e.strength, e.K, r.px_end, r.indirect, r.with_direct,
+                 r.px_begin};
     DeviceWeights w{ctx->d_hash, ctx->d_w32, ctx->d_w32 + ctx->op_t_floats, ctx->op_t_floats, ctx->cn_t_floats};
     launch_relight_fp32(ctx->dims, ctx->hl, w, j, o.clamp_terms, o.kahan, st);
   } else {
@@ -479,24 +512,21 @@ static void relight_one(nwprt_ctx* ctx, const nwprt_request& r, const nwprt_reli
   }
 }
 
-static void relight_many_tc(nwprt_ctx* ctx, const nwprt_request* reqs, int n_reqs,
-                            const nwprt_relight_opts& o, cudaStream_t st) {
+static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, const nwprt_relight_opts& o,
+                            cudaStream_t st) {
   need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
   need(ctx->tc_supported, NWPRT_UNSUPPORTED, ctx->tc_why.c_str());
   std::vector<TcJob> jobs;
   jobs.reserve(n_reqs);
   for (int i = 0; i < n_reqs; ++i) {
-    const nwprt_request& r = reqs[i];
+    RangeReq r = reqs[i];
     EnvEntry& e = env_at(ctx, r.env_id);
-    need(r.frame_id >= 0 && r.frame_id < NWPRT_MAX_FRAMES, NWPRT_INVALID_ARG, "frame id out of range");
+    resolve_range(ctx, r);
     Frame& f = ctx->frames[r.frame_id];
-    need(f.prepared, NWPRT_NOT_READY, "frame was not prepared (call nwprt_prepare first)");
-    check_out(r.indirect, "null indirect output");
-    check_out(r.with_direct, "null with_direct output");
     ensure_emb(ctx, e, st);
-    const int64_t n = (int64_t)f.width * f.height;
-    if (n == 0) continue;
-    jobs.push_back(TcJob{f.packed, f.flag, f.direct, e.emb_k, e.strength, e.K, n, r.indirect, r.with_direct, 0});
+    if (r.px_end == r.px_begin) continue;
+    jobs.push_back(TcJob{f.packed, f.flag, f.direct, e.emb_k, e.strength, e.K, r.px_end, r.indirect, r.with_direct,
+                         0, r.px_begin});
   }
   if (jobs.empty()) return;
   if (ctx->jobs_cap < (int)jobs.size()) {
@@ -510,14 +540,21 @@ static void relight_many_tc(nwprt_ctx* ctx, const nwprt_request* reqs, int n_req
                     ctx->d_jobs, o.kahan, o.clamp_terms, ctx->d_err, st);
 }
 
+static void relight_ranges(nwprt_ctx* ctx, const std::vector<RangeReq>& reqs, const nwprt_relight_opts& o,
+                           cudaStream_t st) {
+  if (o.precision == NWPRT_PREC_BF16) {
+    relight_many_tc(ctx, reqs.data(), (int)reqs.size(), o, st);
+  } else {
+    for (const RangeReq& r : reqs) relight_one(ctx, r, o, st);
+  }
+}
+
 nwprt_status nwprt_relight(nwprt_ctx* ctx, int env_id, int frame_id, const nwprt_relight_opts* opts,
                            float* indirect, float* with_direct, void* stream) {
   return guarded(ctx, [&] {
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
     const nwprt_relight_opts o = opts ? *opts : default_opts();
-    nwprt_request r{env_id, frame_id, indirect, with_direct};
-    if (o.precision == NWPRT_PREC_BF16) relight_many_tc(ctx, &r, 1, o, (cudaStream_t)stream);
-    else relight_one(ctx, r, o, (cudaStream_t)stream);
+    relight_ranges(ctx, {RangeReq{env_id, frame_id, indirect, with_direct, 0, 0}}, o, (cudaStream_t)stream);
   });
 }
 
@@ -526,11 +563,25 @@ nwprt_status nwprt_relight_batch(nwprt_ctx* ctx, const nwprt_request* reqs, int 
   return guarded(ctx, [&] {
     need(ctx && (reqs || n_reqs == 0) && n_reqs >= 0, NWPRT_INVALID_ARG, "bad request list");
     const nwprt_relight_opts o = opts ? *opts : default_opts();
-    if (o.precision == NWPRT_PREC_BF16) {
-      relight_many_tc(ctx, reqs, n_reqs, o, (cudaStream_t)stream);
-    } else {
-      for (int i = 0; i < n_reqs; ++i) relight_one(ctx, reqs[i], o, (cudaStream_t)stream);
-    }
+    std::vector<RangeReq> v;
+    v.reserve(n_reqs);
+    for (int i = 0; i < n_reqs; ++i)
+      v.push_back(RangeReq{reqs[i].env_id, reqs[i].frame_id, reqs[i].indirect, reqs[i].with_direct, 0, 0});
+    relight_ranges(ctx, v, o, (cudaStream_t)stream);
+  });
+}
+
+nwprt_status nwprt_relight_ranges(nwprt_ctx* ctx, const nwprt_range_request* reqs, int n_reqs,
+                                  const nwprt_relight_opts* opts, void* stream) {
+  return guarded(ctx, [&] {
+    need(ctx && (reqs || n_reqs == 0) && n_reqs >= 0, NWPRT_INVALID_ARG, "bad request list");
+    const nwprt_relight_opts o = opts ? *opts : default_opts();
+    std::vector<RangeReq> v;
+    v.reserve(n_reqs);
+    for (int i = 0; i < n_reqs; ++i)
+      v.push_back(RangeReq{reqs[i].env_id, reqs[i].frame_id, reqs[i].indirect, reqs[i].with_direct,
+                           reqs[i].px_begin, reqs[i].px_end});
+    relight_ranges(ctx, v, o, (cudaStream_t)stream);
   });
 }
 
@@ -551,6 +602,10 @@ nwprt_status nwprt_sync(nwprt_ctx* ctx) {
 nwprt_status nwprt_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx, float* strength,
                              void* stream) {
   return guarded(nullptr, [&] { launch_haar_topk(faces, n_env, S, K, idx, strength, nullptr, (cudaStream_t)stream); });
+}
+
+nwprt_status nwprt_env_rotate(const float* src, int S, const float* R, float* dst, void* stream) {
+  return guarded(nullptr, [&] { launch_env_rotate(src, S, R, dst, (cudaStream_t)stream); });
 }
 
 size_t nwprt_sh_project_workspace_size(int S) { return S > 0 ? sh_project_workspace_bytes(S) : 0; }

@@ -108,6 +108,9 @@ void launch_sh_project(const float* faces, int S, float* L, float* workspace, cu
 void launch_sh_dot(const float* T, int64_t n_px, int nc, const float* L, int abs_out, float* out,
                    uint32_t* err, cudaStream_t st);
 
+// env_rotate.cu
+void launch_env_rotate(const float* src, int S, const float* R_host, float* dst, cudaStream_t st);
+
 // relight_common.cu
 void launch_pack_gbuffer(const nwprt_gbuffer& g, float* packed, cudaStream_t st);
 void launch_gather_embedding(const float* emb, int D, int n_coeffs, const int32_t* idx, int K,
@@ -121,9 +124,10 @@ struct RelightJob {
   const float* emb_k;     // [K][D] embedding gathered at the env's indices (FP32)
   const float* strength;  // [K][3]
   int K;
-  int64_t n_px;
+  int64_t n_px;      // end of the pixel range (exclusive)
   float* indirect;
   float* with_direct;
+  int64_t px_begin;  // start of the pixel range
 };
 
 struct DeviceWeights {
@@ -153,10 +157,11 @@ struct TcJob {
   const float* emb_k;     // [K][D] FP32 embedding rows of the env's wavelets
   const float* strength;  // [K][3]
   int K;
-  int64_t n_px;
+  int64_t n_px;           // end of the pixel range (exclusive)
   float* indirect;
   float* with_direct;
   long long tile_begin;   // first 128-pixel tile of this job in the launch (set by the launcher)
+  int64_t px_begin;       // start of the pixel range
 };
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash,
                        const uint16_t* tc_weights_dev, const TcJob* jobs, int n_jobs,

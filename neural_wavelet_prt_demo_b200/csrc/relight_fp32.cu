@@ -34,7 +34,7 @@ struct Fp32Params {
   const float* emb_k;
   const float* strength;
   int K;
-  int64_t n_px;
+  int64_t px_begin, n_px;  // pixel range [px_begin, n_px)
   float* indirect;
   float* with_direct;
   int clamp, kahan;
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(NT, 1) relight_fp32_kernel(Fp32Params p) {
   const int tid = threadIdx.x;
   for (int i = tid * 4; i < p.w_floats; i += NT * 4)
     *reinterpret_cast<float4*>(sW + i) = __ldg(reinterpret_cast<const float4*>(p.w + i));
-  const int64_t px = (int64_t)blockIdx.x * NT + tid;
+  const int64_t px = p.px_begin + (int64_t)blockIdx.x * NT + tid;
   const bool valid = px < p.n_px;
   const bool active = valid && p.flag[px] != 0;
   float* act = sAct + tid;
@@ -242,7 +242,7 @@ bool try_launch(const NetDims& d, const Fp32Params& p, cudaStream_t st) {
   using N256 = Net<D, OPH, OPO, CNH, W, AUXW, 256>;
   using N128 = Net<D, OPH, OPO, CNH, W, AUXW, 128>;
   if (N256::weight_floats() != p.w_floats) fail(NWPRT_INVALID_ARG, "fp32 weight layout mismatch");
-  const int64_t n = p.n_px;
+  const int64_t n = p.n_px - p.px_begin;
   if (N256::smem_bytes(p.w_floats) <= (size_t)max_smem && n >= 256 * 148) {
     auto k = relight_fp32_kernel<N256, D, AUXW, 256>;
     const size_t smem = N256::smem_bytes(p.w_floats);
@@ -292,7 +292,7 @@ bool relight_fp32_supported(const NetDims& d, std::string* why) {
 
 void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWeights& w,
                          const RelightJob& job, int clamp, int kahan, cudaStream_t st) {
-  if (job.n_px == 0) return;
+  if (job.n_px <= job.px_begin) return;
   Fp32Params p;
   p.hl = hl;
   p.hash = w.hash;
@@ -304,6 +304,7 @@ void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWei
   p.emb_k = job.emb_k;
   p.strength = job.strength;
   p.K = job.K;
+  p.px_begin = job.px_begin;
   p.n_px = job.n_px;
   p.indirect = job.indirect;
   p.with_direct = job.with_direct;

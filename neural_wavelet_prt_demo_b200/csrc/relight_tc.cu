@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     const int jid = find_job(p.jobs, p.n_jobs, t);
     const TcJob& J = p.jobs[jid];
     const int K = J.K;
-    const long long px = (t - J.tile_begin) * kTile + row;
+    const long long px = J.px_begin + (t - J.tile_begin) * kTile + row;
     const bool valid = px < J.n_px;
     uint32_t enc[DMAX / 2];
     if (valid) {
@@ -660,7 +660,7 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   long long tiles = 0;
   for (auto& j : J) {
     j.tile_begin = tiles;
-    tiles += (j.n_px + kTile - 1) / kTile;
+    tiles += (j.n_px - j.px_begin + kTile - 1) / kTile;
   }
   if (tiles == 0) return;
   p.total_tiles = tiles;

@@ -32,7 +32,7 @@ from ._lib import NwprtError, check, lib
 from . import netconfig
 
 __all__ = ["RenderEngine", "EnvironmentMap", "FullFrame", "RenderConfig", "NwprtError",
-           "haar_topk", "sh_project", "sh_dot"]
+           "haar_topk", "env_rotate", "sh_project", "sh_dot"]
 
 
 def _ptr(t: Optional[torch.Tensor]):
@@ -301,6 +301,32 @@ class RenderEngine:
         self._check(lib().nwprt_relight_batch(self._ctx, arr, len(requests), C.byref(opts),
                                               _stream_ptr(stream)))
 
+    def relightRanges(self, ranges, config: Optional[RenderConfig] = None, stream=None) -> None:
+        """Pixel-range relights (envMapID, frameID, indirect, with_direct, px_begin, px_end) in
+        one device pass (BF16) -- the primitive the serving loop packs requests into."""
+        config = config or RenderConfig()
+        arr = (_lib.RangeRequest * len(ranges))()
+        for i, (e, fr, ind, wd, b, en) in enumerate(ranges):
+            arr[i] = _lib.RangeRequest(self.envIds[e], fr, ind.data_ptr(), wd.data_ptr(), int(b), int(en))
+        opts = config.opts()
+        self._check(lib().nwprt_relight_ranges(self._ctx, arr, len(ranges), C.byref(opts),
+                                               _stream_ptr(stream)))
+
+    def addEnvironmentFaces(self, faces: torch.Tensor, K: int, stream=None) -> int:
+        """Registers an env map from device-resident faces [6,S,S,3] (Haar + top-K on the GPU)."""
+        if faces.dtype != torch.float32 or not faces.is_cuda or not faces.is_contiguous():
+            raise ValueError("faces must be a contiguous float32 CUDA tensor")
+        env_id = C.c_int(-1)
+        self._check(lib().nwprt_env_from_faces(self._ctx, _ptr(faces), 1, faces.shape[1], int(K),
+                                               _stream_ptr(stream), C.byref(env_id)))
+        self.envIds.append(env_id.value)
+        self.EnvmapSetup = True
+        return len(self.envIds) - 1
+
+    def releaseEnvironmentMap(self, envMapID: int) -> None:
+        self._check(lib().nwprt_env_release(self._ctx, self.envIds[envMapID]))
+        self.envIds[envMapID] = -1
+
     def TCNNSync(self) -> None:
         """tcnn.cu:154-158; also surfaces device-side error reports."""
         self._check(lib().nwprt_sync(self._ctx))
@@ -319,6 +345,18 @@ def haar_topk(faces: torch.Tensor, K: int, stream=None):
     st = torch.empty((E, K, 3), dtype=torch.float32, device=faces.device)
     check(lib().nwprt_haar_topk(_ptr(f), E, S, int(K), _ptr(idx), _ptr(st), _stream_ptr(stream)))
     return (idx, st) if batched else (idx[0], st[0])
+
+
+def env_rotate(faces: torch.Tensor, R, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+    """Rotated cubemap dst(d) = src(R^T d), point-sampled like the reference's env lookup."""
+    if faces.dtype != torch.float32 or not faces.is_cuda or not faces.is_contiguous():
+        raise ValueError("faces must be a contiguous float32 CUDA tensor")
+    r = np.ascontiguousarray(np.asarray(R, np.float32).reshape(9))
+    if out is None:
+        out = torch.empty_like(faces)
+    check(lib().nwprt_env_rotate(_ptr(faces), faces.shape[1], r.ctypes.data_as(C.c_void_p), _ptr(out),
+                                 _stream_ptr(stream)))
+    return out
 
 
 def sh_project(faces: torch.Tensor, stream=None) -> torch.Tensor:

@@ -1,0 +1,328 @@
+"""Continuous-batching relight server.
+
+Requests of mixed resolution, K and env map arrive over time.  The server keeps the
+network weights and the G-buffers of every resolution resident in HBM, admits requests
+while a device-memory budget allows (their output buffers and env tables), and feeds the
+GPU fixed-size *quanta* of work: each quantum is one ``nwprt_relight_ranges`` launch that
+packs 128-pixel-aligned pixel ranges of several admitted requests, smallest remaining
+work first.  Requests that arrive while quanta are running join the next quantum, so
+large requests never block small ones for longer than one quantum, and two quanta are
+kept in flight so the GPU does not idle while the host forms the next one.
+
+Each request's env map is either new cubemap faces (Haar + top-K on the GPU) or a
+rotation of a resident map (``env_rotate`` then Haar + top-K), stream-ordered ahead of
+the request's first quantum.  The reference renders one frame at a time behind a 2-frame
+ping-pong (Renderer/OutputVisualizer.cpp:61-126); this generalises that overlap to many
+concurrent requests.
+
+``plan_quantum`` / ``Admission`` are pure host logic (tested on CPU); ``RelightServer``
+drives the GPU.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Deque, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+TILE = 128          # pixels per tensor-core tile; quanta split requests on tile boundaries
+OUT_BYTES_PER_PX = 32  # two float4 outputs
+
+
+# ---------------------------------------------------------------------------- requests
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float            # seconds after the stream starts
+    res: int                  # index of the resident frame (resolution)
+    K: int                    # wavelets
+    env_kind: str             # "new" (faces given) or "rot" (rotation of a resident env map)
+    faces: Optional[np.ndarray] = None   # [6,S,S,3] for "new"
+    base_env: int = -1                   # resident env index for "rot"
+    R: Optional[np.ndarray] = None       # 3x3 rotation for "rot"
+    # filled by the server (max_queue_s: longest a request may wait for admission)
+    n_px: int = 0
+    next_px: int = 0
+    status: str = "pending"   # pending -> queued -> active -> done | rejected | timeout | error
+    t_admit: float = math.nan
+    t_done: float = math.nan
+    env_id: int = -1
+    bytes_held: int = 0
+    outputs: Tuple = ()
+
+    @property
+    def remaining_evals(self) -> int:
+        return (self.n_px - self.next_px) * self.K
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.arrival
+
+
+def request_bytes(n_px: int, K: int, face_size: int, enc_dims: int) -> int:
+    """Device bytes a request holds while admitted: outputs, env table, rotated faces."""
+    return n_px * OUT_BYTES_PER_PX + K * (4 + 12 + 4 * enc_dims) + 6 * face_size * face_size * 12
+
+
+class Admission:
+    """Admits queued requests first-come first-served while the byte budget allows."""
+
+    def __init__(self, budget_bytes: int):
+        self.budget = int(budget_bytes)
+        self.used = 0
+
+    def fits(self, nbytes: int) -> bool:
+        return self.used + nbytes <= self.budget
+
+    def take(self, nbytes: int) -> None:
+        if not self.fits(nbytes):
+            raise RuntimeError("admission over budget")
+        self.used += nbytes
+
+    def give(self, nbytes: int) -> None:
+        self.used -= nbytes
+        assert self.used >= 0
+
+
+def plan_quantum(active: Sequence[Request], quantum_evals: int) -> List[Tuple[Request, int, int]]:
+    """Chunks for one launch: requests in order of least remaining work, each chunk a
+    128-pixel-aligned range, until the quantum is full.  Always makes progress: the first
+    request gets at least one tile even if that alone exceeds the quantum."""
+    plan = []
+    used = 0
+    for r in sorted((r for r in active if r.next_px < r.n_px), key=lambda r: (r.remaining_evals, r.rid)):
+        room = quantum_evals - used
+        if room <= 0 and plan:
+            break
+        tiles = max(1, room // (TILE * r.K))
+        end = min(r.n_px, r.next_px + tiles * TILE)
+        if end <= r.next_px:
+            continue
+        plan.append((r, r.next_px, end))
+        used += (end - r.next_px) * r.K
+    return plan
+
+
+def percentile(xs: Sequence[float], q: float) -> float:
+    if not len(xs):
+        return math.nan
+    return float(np.percentile(np.asarray(xs, np.float64), q))
+
+
+# ---------------------------------------------------------------------------- stream
+
+RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080), (2560, 1440)]
+KS = [64, 128, 300]
+
+
+def random_rotation(g: np.random.Generator) -> np.ndarray:
+    """Uniform rotation from a uniform unit quaternion (Shoemake's method)."""
+    u1, u2, u3 = g.uniform(size=3)
+    q = np.array([math.sqrt(1 - u1) * math.sin(2 * math.pi * u2), math.sqrt(1 - u1) * math.cos(2 * math.pi * u2),
+                  math.sqrt(u1) * math.sin(2 * math.pi * u3), math.sqrt(u1) * math.cos(2 * math.pi * u3)])
+    x, y, z, w = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]], np.float32)
+
+
+def make_stream(n: int, rate: float, seed: int = 0, face_size: int = 64, p_new: float = 0.4,
+                n_base_envs: int = 8, resolutions=RESOLUTIONS, ks=KS) -> List[Request]:
+    """The serving workload: Poisson arrivals at `rate`/s, resolution and K uniform,
+    `p_new` new log-normal env maps, the rest random rotations of resident maps."""
+    from .synth import make_env_faces
+    g = np.random.Generator(np.random.PCG64([seed, 77]))
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += g.exponential(1.0 / rate)
+        res = int(g.integers(len(resolutions)))
+        K = int(ks[int(g.integers(len(ks)))])
+        if g.uniform() < p_new:
+            faces = make_env_faces(face_size, seed=seed, index=1000 + i)
+            out.append(Request(i, t, res, K, "new", faces=faces))
+        else:
+            out.append(Request(i, t, res, K, "rot", base_env=int(g.integers(n_base_envs)), R=random_rotation(g)))
+    return out
+
+
+# ---------------------------------------------------------------------------- GPU server
+
+class RelightServer:
+    """Serves a list of requests in real time on one GPU through one RenderEngine."""
+
+    def __init__(self, engine, frames, base_faces, precision: str = "bf16", budget_bytes: int = 150 << 30,
+                 quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
+                 max_in_flight: int = 2, keep_outputs: bool = False):
+        import torch
+        self.torch = torch
+        self.e = engine
+        self.frames = frames            # resident FullFrame per resolution index (TCNNPass_p1 done)
+        self.base_faces = base_faces    # device faces of the resident env maps, [6,S,S,3] each
+        from .engine import RenderConfig
+        self.cfg = RenderConfig(precision=precision)
+        self.adm = Admission(budget_bytes)
+        self.quantum = int(est_evals_per_s * quantum_ms / 1e3)
+        self.max_queue_s = max_queue_s
+        self.max_in_flight = max_in_flight
+        self.keep_outputs = keep_outputs
+        self.stream = torch.cuda.current_stream()
+        info = engine.networkInfo()
+        self.face_size, self.enc_dims = info.face_size, info.enc_dims
+        self.quanta = 0
+        self.max_active = 0
+
+    def _prepare(self, r: Request) -> None:
+        """Output buffers and the env wavelet table, stream-ordered before its first quantum."""
+        torch = self.torch
+        fr = self.frames[r.res]
+        ind = torch.empty((r.n_px, 4), dtype=torch.float32, device=fr.fbPredictedIndirect.device)
+        wd = torch.empty_like(ind)
+        if r.env_kind == "new":
+            faces = torch.from_numpy(np.ascontiguousarray(r.faces, np.float32)).to(ind.device, non_blocking=True)
+        elif r.env_kind == "rot":
+            from .engine import env_rotate
+            faces = env_rotate(self.base_faces[r.base_env], r.R)
+        else:
+            raise ValueError(f"unknown env kind {r.env_kind!r}")
+        r.env_id = self.e.addEnvironmentFaces(faces, r.K)
+        r.outputs = (ind, wd, faces)
+
+    def run(self, requests: List[Request], realtime: bool = True) -> Dict:
+        torch = self.torch
+        pending: Deque[Request] = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
+        queue: Deque[Request] = deque()
+        active: List[Request] = []
+        in_flight: Deque[Tuple] = deque()
+        for r in requests:
+            fr = self.frames[r.res]
+            r.n_px = fr.width * fr.height
+            r.next_px = 0
+            r.status = "pending"
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+        finished = 0
+        total = len(requests)
+        while finished < total:
+            t = now() if realtime else math.inf
+            while pending and pending[0].arrival <= t:
+                r = pending.popleft()
+                r.status = "queued"
+                queue.append(r)
+            # admission (FCFS under the byte budget; over-budget and stale requests are refused)
+            while queue:
+                r = queue[0]
+                nbytes = request_bytes(r.n_px, r.K, self.face_size, self.enc_dims)
+                if nbytes > self.adm.budget:
+                    queue.popleft()
+                    r.status, r.t_done = "rejected", now()
+                    finished += 1
+                    continue
+                if not self.adm.fits(nbytes):
+                    if realtime and now() - r.arrival > self.max_queue_s:
+                        queue.popleft()
+                        r.status, r.t_done = "timeout", now()
+                        finished += 1
+                        continue
+                    break
+                queue.popleft()
+                try:
+                    self._prepare(r)
+                except Exception:
+                    r.status, r.t_done = "error", now()
+                    finished += 1
+                    continue
+                self.adm.take(nbytes)
+                r.bytes_held = nbytes
+                r.status, r.t_admit = "active", now()
+                active.append(r)
+            self.max_active = max(self.max_active, len(active))
+            if active and len(in_flight) < self.max_in_flight:
+                plan = plan_quantum(active, self.quantum)
+                ranges = []
+                for r, b, e in plan:
+                    ranges.append((r.env_id, r.res, r.outputs[0], r.outputs[1], b, e))
+                    r.next_px = e
+                self.e.relightRanges(ranges, self.cfg)
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                done_now = [r for r, _, _ in plan if r.next_px >= r.n_px]
+                for r in done_now:
+                    active.remove(r)
+                in_flight.append((ev, done_now))
+                self.quanta += 1
+                continue
+            if in_flight:
+                ev, done_now = in_flight.popleft()
+                ev.synchronize()
+                t = now()
+                for r in done_now:
+                    r.status, r.t_done = "done", t
+                    self.adm.give(r.bytes_held)
+                    self.e.releaseEnvironmentMap(r.env_id)
+                    if not self.keep_outputs:
+                        r.outputs = ()
+                    finished += 1
+                continue
+            if pending:
+                if realtime:
+                    dt = pending[0].arrival - now()
+                    if dt > 0:
+                        time.sleep(min(dt, 0.002))
+                continue
+            if queue:  # nothing active, nothing in flight, but the head does not fit: cannot happen
+                raise RuntimeError("admission stalled")
+        self.e.TCNNSync()
+        return summarize(requests, now())
+
+
+def summarize(requests: Sequence[Request], makespan: float) -> Dict:
+    done = [r for r in requests if r.status == "done"]
+    lat = [r.latency * 1e3 for r in done]
+    evals = sum(r.n_px * r.K for r in done)
+    return {
+        "requests": len(requests),
+        "done": len(done),
+        "rejected": sum(r.status == "rejected" for r in requests),
+        "timeout": sum(r.status == "timeout" for r in requests),
+        "error": sum(r.status == "error" for r in requests),
+        "makespan_s": makespan,
+        "evals_per_s": evals / makespan if makespan > 0 else math.nan,
+        "p50_ms": percentile(lat, 50),
+        "p99_ms": percentile(lat, 99),
+        "max_ms": max(lat) if lat else math.nan,
+    }
+
+
+def serve_serial(engine, frames, base_faces, requests: List[Request], precision: str = "fp32",
+                 realtime: bool = True) -> Dict:
+    """Baseline: one request at a time in arrival order, each a whole-frame relight."""
+    import torch
+    from .engine import RenderConfig, env_rotate
+    cfg = RenderConfig(precision=precision)
+    t0 = time.perf_counter()
+    now = lambda: time.perf_counter() - t0
+    for r in sorted(requests, key=lambda r: (r.arrival, r.rid)):
+        if realtime:
+            while now() < r.arrival:
+                time.sleep(min(r.arrival - now(), 0.002))
+        fr = frames[r.res]
+        r.n_px = fr.width * fr.height
+        if r.env_kind == "new":
+            faces = torch.from_numpy(np.ascontiguousarray(r.faces, np.float32)).to(fr.fbPredictedIndirect.device)
+        else:
+            faces = env_rotate(base_faces[r.base_env], r.R)
+        env = engine.addEnvironmentFaces(faces, r.K)
+        out = torch.empty((r.n_px, 4), dtype=torch.float32, device=faces.device)
+        out2 = torch.empty_like(out)
+        engine.relightRanges([(env, r.res, out, out2, 0, r.n_px)], cfg)
+        torch.cuda.synchronize()
+        r.status, r.t_done = "done", now()
+        r.outputs = (out, out2, faces)
+        engine.releaseEnvironmentMap(env)
+    engine.TCNNSync()
+    return summarize(requests, now())

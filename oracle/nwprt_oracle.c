@@ -595,3 +595,52 @@ int orc_relight_f64(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
   }
   return bad ? -1 : 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Env-map rotation (point-sampled cubemap lookup, cubeMap.cu:23-113)        */
+/* ------------------------------------------------------------------------ */
+
+/* dst texel (f, r, c) = src texel seen in direction R^T d, d = EnvUVToDirec of the
+ * texel centre (unnormalised), face/uv by EnvDirecToUV with its six tests applied in
+ * order (a later match overrides), point sampling with wrap addressing.  FP32 ops
+ * without contraction, in the same order as the GPU kernel. */
+void orc_env_rotate(const float* src, int S, const float R[9], float* dst) {
+  const float fs = (float)S;
+  for (int f = 0; f < 6; ++f)
+    for (int r = 0; r < S; ++r)
+      for (int c = 0; c < S; ++c) {
+        const float uc = 2.f * (((float)c + 0.5f) / fs) - 1.f;
+        const float vc = 2.f * (((float)r + 0.5f) / fs) - 1.f;
+        float x, y, z;
+        switch (f) {
+          case 0: x = 1.f; y = vc; z = uc; break;
+          case 1: x = -1.f; y = vc; z = -uc; break;
+          case 2: x = uc; y = 1.f; z = vc; break;
+          case 3: x = uc; y = -1.f; z = -vc; break;
+          case 4: x = uc; y = vc; z = -1.f; break;
+          default: x = -uc; y = vc; z = 1.f; break;
+        }
+        const float sx = (R[0] * x + R[3] * y) + R[6] * z;
+        const float sy = (R[1] * x + R[4] * y) + R[7] * z;
+        const float sz = (R[2] * x + R[5] * y) + R[8] * z;
+        const float ax = fabsf(sx), ay = fabsf(sy), az = fabsf(sz);
+        float maxa = 1.f, su = 0.f, sv = 0.f;
+        int sf = 0;
+        if (sx > 0.f && ax >= ay && ax >= az) { maxa = ax; su = sz; sv = sy; sf = 0; }
+        if (!(sx > 0.f) && ax >= ay && ax >= az) { maxa = ax; su = -sz; sv = sy; sf = 1; }
+        if (sy > 0.f && ay >= ax && ay >= az) { maxa = ay; su = sx; sv = sz; sf = 2; }
+        if (!(sy > 0.f) && ay >= ax && ay >= az) { maxa = ay; su = sx; sv = -sz; sf = 3; }
+        if (!(sz > 0.f) && az >= ax && az >= ay) { maxa = az; su = sx; sv = sy; sf = 4; }
+        if (sz > 0.f && az >= ax && az >= ay) { maxa = az; su = -sx; sv = sy; sf = 5; }
+        if (!(maxa > 0.f)) { maxa = 1.f; su = -1.f; sv = -1.f; sf = 0; }
+        const float u = 0.5f * (su / maxa + 1.f);
+        const float v = 0.5f * (sv / maxa + 1.f);
+        int col = (int)floorf(u * fs) % S;
+        int row = (int)floorf(v * fs) % S;
+        if (col < 0) col += S;
+        if (row < 0) row += S;
+        const float* s = src + (((int64_t)sf * S + row) * S + col) * 3;
+        float* d = dst + (((int64_t)f * S + r) * S + c) * 3;
+        d[0] = s[0]; d[1] = s[1]; d[2] = s[2];
+      }
+}

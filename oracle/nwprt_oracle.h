@@ -67,6 +67,9 @@ int orc_haar_topk(const float* faces, int S, int K, int32_t* idx, float* strengt
 int orc_haar_topk_batch(const float* faces, int n_env, int S, int K, int32_t* idx,
                         float* strength, int n_threads);
 
+/* ---- env-map rotation (point-sampled, as the reference's cubemap lookup) ---- */
+void orc_env_rotate(const float* src, int S, const float R[9], float* dst);
+
 /* ---- SH baseline ---- */
 void orc_sh_eval_f64(double x, double y, double z, int lmax, double* out);
 void orc_sh_project_f64(const float* faces, int S, int lmax, double* L, double* L_abs);

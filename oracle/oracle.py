@@ -149,6 +149,14 @@ def haar_topk(faces: np.ndarray, K: int, n_threads: int = 0):
     return (idx, st) if batched else (idx[0], st[0])
 
 
+def env_rotate(faces: np.ndarray, R: np.ndarray) -> np.ndarray:
+    f = np.ascontiguousarray(faces, np.float32)
+    r = np.ascontiguousarray(np.asarray(R, np.float32).reshape(9))
+    out = np.empty_like(f)
+    lib().orc_env_rotate(_p(f), C.c_int(f.shape[1]), _p(r), _p(out))
+    return out
+
+
 def sh_eval_f64(d, lmax=8) -> np.ndarray:
     out = np.zeros((lmax + 1) ** 2, np.float64)
     lib().orc_sh_eval_f64(C.c_double(d[0]), C.c_double(d[1]), C.c_double(d[2]), C.c_int(lmax),

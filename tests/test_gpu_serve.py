@@ -1,0 +1,158 @@
+"""GPU tests of the serving path: env-map rotation parity, pixel-range relights and the
+continuous-batching server (results inside the mix equal results relit alone, bitwise;
+admission under a memory budget; rejection, timeout and error paths)."""
+import numpy as np
+import pytest
+
+from neural_wavelet_prt_demo_b200 import netconfig, serve, synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _eng():
+    from neural_wavelet_prt_demo_b200 import engine
+    return engine
+
+
+def test_env_rotate_bit_exact_and_identity(cuda):
+    import torch
+    eng = _eng()
+    g = np.random.default_rng(0)
+    for S in (1, 8, 64, 128):
+        faces = synth.make_env_faces(S, seed=S)
+        tf = torch.from_numpy(faces).to(cuda)
+        assert torch.equal(eng.env_rotate(tf, np.eye(3)), tf)
+        for _ in range(3):
+            R = serve.random_rotation(g)
+            got = eng.env_rotate(tf, R).cpu().numpy()
+            assert np.array_equal(got.view(np.uint32), O.env_rotate(faces, R).view(np.uint32))
+    # axis permutations land texels on texels exactly
+    R = np.array([[0, 0, 1], [0, 1, 0], [-1, 0, 0]], np.float32)
+    faces = synth.make_env_faces(16, seed=3)
+    got = eng.env_rotate(torch.from_numpy(faces).to(cuda), R).cpu().numpy()
+    assert np.array_equal(got, O.env_rotate(faces, R))
+    with pytest.raises(eng.NwprtError):
+        eng.env_rotate(torch.from_numpy(faces).to(cuda), np.full((3, 3), np.nan))
+
+
+@pytest.fixture(scope="module")
+def rig(cuda):
+    import torch
+    eng = _eng()
+    desc = netconfig.parse(netconfig.CONFIG_LARGE)
+    w = synth.make_weights(desc, seed=0, hash_scale=0.5, param_round="fp16")
+    e = eng.RenderEngine(netconfig.CONFIG_LARGE)
+    e.loadWeights(w)
+    sizes = [(64, 48), (100, 37), (128, 128)]
+    frames = []
+    for i, (W, H) in enumerate(sizes):
+        fr = eng.FullFrame.from_gbuffer(synth.make_gbuffer(W, H, seed=50 + i, flag_prob=0.9), cuda)
+        e.setFrame(i, fr)
+        e.TCNNPass_p1(i)
+        frames.append(fr)
+    base = [torch.from_numpy(synth.make_env_faces(64, seed=60, index=j)).to(cuda) for j in range(3)]
+    yield e, frames, base
+    e.close()
+
+
+def _requests(n, seed=0, spacing=0.003):
+    g = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        res, K = int(g.integers(3)), int(g.choice([16, 64, 100, 300]))
+        if g.uniform() < 0.4:
+            out.append(serve.Request(i, i * spacing, res, K, "new",
+                                     faces=synth.make_env_faces(64, seed=seed, index=500 + i)))
+        else:
+            out.append(serve.Request(i, i * spacing, res, K, "rot", base_env=int(g.integers(3)),
+                                     R=serve.random_rotation(g)))
+    return out
+
+
+def _solo(e, frames, base, r):
+    import torch
+    eng = _eng()
+    fr = frames[r.res]
+    faces = (torch.from_numpy(r.faces).to(fr.fbPredictedIndirect.device) if r.env_kind == "new"
+             else eng.env_rotate(base[r.base_env], r.R))
+    env = e.addEnvironmentFaces(faces, r.K)
+    n = fr.width * fr.height
+    out, out2 = torch.empty((n, 4), device=faces.device), torch.empty((n, 4), device=faces.device)
+    e.relightRanges([(env, r.res, out, out2, 0, n)], eng.RenderConfig(precision="bf16"))
+    e.TCNNSync()
+    e.releaseEnvironmentMap(env)
+    return out, out2
+
+
+def test_pixel_ranges_compose_to_the_whole_frame(rig):
+    import torch
+    e, frames, base = rig
+    eng = _eng()
+    r = _requests(1, seed=4)[0]
+    r.res = 2
+    ref, ref2 = _solo(e, frames, base, r)
+    faces = (torch.from_numpy(r.faces).cuda() if r.env_kind == "new" else eng.env_rotate(base[r.base_env], r.R))
+    env = e.addEnvironmentFaces(faces, r.K)
+    n = frames[2].width * frames[2].height
+    out, out2 = torch.zeros((n, 4), device="cuda"), torch.zeros((n, 4), device="cuda")
+    cuts = [0, 128, 128 * 37, 128 * 90, n]
+    e.relightRanges([(env, 2, out, out2, cuts[i], cuts[i + 1]) for i in range(len(cuts) - 1)],
+                    eng.RenderConfig(precision="bf16"))
+    e.TCNNSync()
+    assert torch.equal(out, ref) and torch.equal(out2, ref2)
+    with pytest.raises(eng.NwprtError):
+        e.relightRanges([(env, 2, out, out2, 0, n + 1)], eng.RenderConfig(precision="bf16"))
+    e.releaseEnvironmentMap(env)
+
+
+def test_served_results_equal_solo_results(rig):
+    import torch
+    e, frames, base = rig
+    reqs = _requests(14, seed=1)
+    srv = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=0.05, est_evals_per_s=9e9,
+                              keep_outputs=True)
+    stats = srv.run(reqs)
+    assert stats["done"] == len(reqs), stats
+    assert srv.quanta > len(reqs)          # requests were split across several launches
+    for r in reqs:
+        ind, wd = _solo(e, frames, base, r)
+        assert torch.equal(r.outputs[0], ind), r.rid
+        assert torch.equal(r.outputs[1], wd), r.rid
+        assert r.latency >= 0
+
+
+def test_budget_admits_one_request_at_a_time(rig):
+    e, frames, base = rig
+    reqs = _requests(6, seed=2, spacing=0.0)
+    for r in reqs:
+        r.res, r.K = 2, 300
+    one = serve.request_bytes(frames[2].width * frames[2].height, 300, 64, 32)
+    srv = serve.RelightServer(e, frames, base, budget_bytes=one + one // 2, quantum_ms=0.2)
+    stats = srv.run(reqs)
+    assert stats["done"] == 6 and srv.max_active == 1
+
+
+def test_rejection_timeout_and_error_paths(rig):
+    e, frames, base = rig
+    reqs = _requests(5, seed=3, spacing=0.0)
+    # a request larger than the whole budget is refused; the others are served
+    small = serve.request_bytes(frames[0].width * frames[0].height, 300, 64, 32)
+    for r in reqs:
+        r.res = 0
+    reqs[2].res = 2
+    srv = serve.RelightServer(e, frames, base, budget_bytes=small, quantum_ms=0.2)
+    stats = srv.run(reqs)
+    assert reqs[2].status == "rejected" and stats["rejected"] == 1 and stats["done"] == 4
+    # malformed env map (wrong face size) fails that request only
+    reqs = _requests(4, seed=5, spacing=0.0)
+    reqs[1].env_kind, reqs[1].faces = "new", synth.make_env_faces(16, seed=1)
+    stats = serve.RelightServer(e, frames, base, quantum_ms=0.2).run(reqs)
+    assert reqs[1].status == "error" and stats["done"] == 3
+    # a queue deadline of zero with room for one request at a time times the rest out
+    reqs = _requests(5, seed=6, spacing=0.0)
+    for r in reqs:
+        r.res, r.K = 2, 300
+    one = serve.request_bytes(frames[2].width * frames[2].height, 300, 64, 32)
+    stats = serve.RelightServer(e, frames, base, budget_bytes=one, quantum_ms=0.2, max_queue_s=0.0).run(reqs)
+    assert stats["timeout"] >= 1 and stats["done"] >= 1 and stats["done"] + stats["timeout"] == 5

@@ -1,0 +1,78 @@
+"""CPU tests of the serving policy: quantum planning, admission, the request stream."""
+import math
+
+import numpy as np
+import pytest
+
+from neural_wavelet_prt_demo_b200 import serve
+
+
+def _req(rid, n_px, K, next_px=0):
+    r = serve.Request(rid, 0.0, 0, K, "rot")
+    r.n_px, r.next_px = n_px, next_px
+    return r
+
+
+def test_quantum_is_tile_aligned_srpt_and_bounded():
+    active = [_req(0, 1920 * 1080, 300), _req(1, 256 * 256, 64), _req(2, 512 * 512, 128, next_px=128 * 100)]
+    q = 50_000_000
+    plan = serve.plan_quantum(active, q)
+    assert [r.rid for r, _, _ in plan] == [1, 2, 0]          # least remaining work first
+    for r, b, e in plan:
+        assert b == r.next_px and e > b
+        assert b % serve.TILE == 0 and (e % serve.TILE == 0 or e == r.n_px)
+    used = sum((e - b) * r.K for r, b, e in plan)
+    assert used <= q
+
+
+def test_quantum_always_progresses_and_finishes_requests():
+    r = _req(0, 1000, 300)
+    plans = 0
+    while r.next_px < r.n_px:
+        plan = serve.plan_quantum([r], quantum_evals=1)      # smaller than one tile
+        assert len(plan) == 1
+        _, b, e = plan[0]
+        assert e - b == min(serve.TILE, r.n_px - b)
+        r.next_px = e
+        plans += 1
+    assert plans == math.ceil(1000 / serve.TILE)
+    assert serve.plan_quantum([r], 10 ** 9) == []
+
+
+def test_admission_budget():
+    a = serve.Admission(100)
+    assert a.fits(60)
+    a.take(60)
+    assert not a.fits(41) and a.fits(40)
+    with pytest.raises(RuntimeError):
+        a.take(41)
+    a.give(60)
+    assert a.used == 0
+
+
+def test_request_bytes_counts_outputs_and_env_table():
+    assert serve.request_bytes(100, 10, 64, 32) == 100 * 32 + 10 * (4 + 12 + 128) + 6 * 64 * 64 * 12
+
+
+def test_stream_is_seeded_poisson_with_the_configured_mix():
+    reqs = serve.make_stream(2000, 120.0, seed=0, face_size=4)
+    assert [r.rid for r in reqs] == list(range(2000))
+    gaps = np.diff([0.0] + [r.arrival for r in reqs])
+    assert abs(gaps.mean() - 1 / 120) < 0.1 / 120
+    frac_new = np.mean([r.env_kind == "new" for r in reqs])
+    assert abs(frac_new - 0.4) < 0.05
+    assert {r.K for r in reqs} == {64, 128, 300}
+    assert {r.res for r in reqs} == set(range(5))
+    for r in reqs[:50]:
+        if r.env_kind == "rot":
+            assert np.allclose(r.R @ r.R.T, np.eye(3), atol=1e-5) and abs(np.linalg.det(r.R) - 1) < 1e-5
+    again = serve.make_stream(20, 120.0, seed=0, face_size=4)
+    assert [(r.arrival, r.res, r.K, r.env_kind) for r in again] == [(r.arrival, r.res, r.K, r.env_kind) for r in reqs[:20]]
+
+
+def test_summary_percentiles():
+    reqs = [serve.Request(i, 0.0, 0, 1, "rot") for i in range(100)]
+    for i, r in enumerate(reqs):
+        r.status, r.t_done, r.n_px = "done", (i + 1) / 1000.0, 1
+    s = serve.summarize(reqs, 1.0)
+    assert s["done"] == 100 and abs(s["p50_ms"] - 50.5) < 1e-9 and abs(s["p99_ms"] - 99.01) < 1e-9
