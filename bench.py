@@ -41,7 +41,11 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["auto", "bf16", "fp32"], default="auto")
-    ap.add_argument("--workload", choices=["relight1080", "sh1080"], default="relight1080")
+    ap.add_argument("--workload", choices=["relight1080", "sh1080", "serve"], default="relight1080")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=120.0)
+    ap.add_argument("--serve-serial-prefix", type=int, default=40,
+                    help="requests of the stream also served by the plain FP32 serial baseline")
     ap.add_argument("--fp32-steps", type=int, default=2, help="timed steps of the plain FP32 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -161,6 +165,8 @@ def run_ours(args):
 
     if args.workload == "sh1080":
         return run_sh(args, rank, world, local, dev)
+    if args.workload == "serve":
+        return run_serve(args, rank, world, local, dev)
 
     desc, w, gb, faces = make_relight_inputs(rank)
     e = eng.RenderEngine(netconfig_json(), device=local)
@@ -356,6 +362,95 @@ def run_sh(args, rank, world, local, dev):
                           "gpu_launches": args.steps}), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------- serving stream
+
+def _serve_rig(cfg, face_size, dev, seed=0):
+    import torch
+    from neural_wavelet_prt_demo_b200 import engine as eng, netconfig, serve, synth
+    desc = netconfig.parse(cfg)
+    w = synth.make_weights(desc, seed=seed, hash_scale=1e-4,
+                           param_round="fp16" if cfg is netconfig.CONFIG_LARGE else "fp32")
+    e = eng.RenderEngine(cfg, device=dev.index or 0)
+    e.loadWeights(w)
+    frames = []
+    for i, (W, H) in enumerate(serve.RESOLUTIONS):
+        fr = eng.FullFrame.from_gbuffer(synth.make_gbuffer(W, H, seed=200 + i), dev)
+        e.setFrame(i, fr)
+        e.TCNNPass_p1(i)
+        frames.append(fr)
+    base = [torch.from_numpy(synth.make_env_faces(face_size, seed=300, index=j)).to(dev) for j in range(8)]
+    torch.cuda.synchronize()
+    return e, frames, base
+
+
+def _measure_rate(e, frames, base, precision):
+    """Steady-state evals/s of one 1080p K=300 relight (sizes the scheduling quantum)."""
+    import torch
+    from neural_wavelet_prt_demo_b200 import engine as eng
+    env = e.addEnvironmentFaces(base[0], 300)
+    fr = frames[3]
+    n = fr.width * fr.height
+    out, out2 = torch.empty((n, 4), device=base[0].device), torch.empty((n, 4), device=base[0].device)
+    cfg = eng.RenderConfig(precision=precision)
+    e.relightRanges([(env, 3, out, out2, 0, n)], cfg)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    e.relightRanges([(env, 3, out, out2, 0, n)], cfg)
+    b.record()
+    torch.cuda.synchronize()
+    e.releaseEnvironmentMap(env)
+    return n * 300 / (a.elapsed_time(b) / 1e3)
+
+
+def run_serve(args, rank, world, local, dev):
+    """Config-4 serving stream: Poisson arrivals, mixed resolution / K / env maps (40% new,
+    60% rotations of resident maps), budget admission, continuous batching.  Reports
+    throughput and p50/p99 latency of the served BF16 path, the same for a small (config-0)
+    network, and the plain FP32 serial baseline on a prefix of the stream."""
+    import torch
+    from neural_wavelet_prt_demo_b200 import netconfig, serve
+    out = {}
+    sampler = ClockSampler(local)
+    for name, cfg, S in (("served_bf16", netconfig.CONFIG_LARGE, 64),
+                         ("served_bf16_small_net", netconfig.CONFIG_SMALL, 32)):
+        e, frames, base = _serve_rig(cfg, S, dev)
+        rate = _measure_rate(e, frames, base, "bf16")
+        reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=rank, face_size=S)
+        srv = serve.RelightServer(e, frames, base, precision="bf16", budget_bytes=150 << 30, quantum_ms=12.0,
+                                  est_evals_per_s=rate)
+        if name == "served_bf16":
+            sampler.start()
+        st = srv.run(reqs)
+        if name == "served_bf16":
+            clocks = sampler.stop()
+        st.update({"quanta": srv.quanta, "max_concurrent": srv.max_active, "kernel_evals_per_s_1080p": rate,
+                   "offered_evals_per_s": sum(r.n_px * r.K for r in reqs) / reqs[-1].arrival})
+        out[name] = st
+        if name == "served_bf16" and args.serve_serial_prefix > 0:
+            m = args.serve_serial_prefix
+            prefix = serve.make_stream(m, args.serve_rate, seed=rank, face_size=S)
+            st2 = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=12.0,
+                                      est_evals_per_s=rate).run(prefix)
+            out["served_bf16_prefix"] = st2
+            prefix = serve.make_stream(m, args.serve_rate, seed=rank, face_size=S)
+            out["serial_fp32_prefix"] = serve.serve_serial(e, frames, base, prefix, precision="fp32")
+        e.close()
+        del frames, base
+        torch.cuda.empty_cache()
+    if rank == 0:
+        s = out["served_bf16"]
+        line = {"metric": f"p99 relight latency, {args.serve_requests} requests Poisson {args.serve_rate:g}/s",
+                "value": s["p99_ms"], "unit": "ms", "n_gpus": world, "steps": 1, "warmup": 0,
+                "ms_per_step": s["makespan_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+                "config": {"workload": "serving stream: resolutions {256^2, 512^2, 720p, 1080p, 1440p}, "
+                                       "K in {64,128,300}, 40% new 6x64x64 env maps, 60% rotations, "
+                                       "150 GB admission budget, 12 ms quanta"},
+                "clocks": clocks, **out}
+        print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------- reference arm
