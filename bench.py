@@ -41,7 +41,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["auto", "bf16", "fp32"], default="auto")
-    ap.add_argument("--workload", choices=["relight1080", "sh1080", "serve"], default="relight1080")
+    ap.add_argument("--workload", choices=["relight1080", "sh1080", "serve", "sweep"], default="relight1080")
+    ap.add_argument("--sweep-px", type=int, default=4096, help="pixels checked against the FP64 oracle per K")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=120.0)
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
@@ -167,6 +168,8 @@ def run_ours(args):
         return run_sh(args, rank, world, local, dev)
     if args.workload == "serve":
         return run_serve(args, rank, world, local, dev)
+    if args.workload == "sweep":
+        return run_sweep(args, rank, world, local, dev)
 
     desc, w, gb, faces = make_relight_inputs(rank)
     e = eng.RenderEngine(netconfig_json(), device=local)
@@ -451,6 +454,61 @@ def run_serve(args, rank, world, local, dev):
                                        "150 GB admission budget, 12 ms quanta"},
                 "clocks": clocks, **out}
         print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- precision sweep
+
+def run_sweep(args, rank, world, local, dev):
+    """Config-3 precision sweep: the 1080p frame relit at K in {128, 300, 512} in BF16 and in
+    FP32; per K, throughput and max / mean relative error and PSNR against the FP64 oracle of
+    the same network and weights on a pixel sample spread over the frame."""
+    import torch
+    from neural_wavelet_prt_demo_b200 import engine as eng
+    from oracle import oracle as O
+    desc, w, gb, faces = make_relight_inputs(rank)
+    e = eng.RenderEngine(netconfig_json(), device=local)
+    e.loadWeights(w)
+    fr = eng.FullFrame.from_gbuffer(gb, dev)
+    e.setFrame(0, fr)
+    e.TCNNPass_p1(0)
+    b = O.Bound(desc, w, gb)
+    N = gb.n
+    # sample: args.sweep_px pixels in 16 contiguous runs spread over the frame
+    runs, per = 16, max(1, args.sweep_px // 16)
+    starts = [int(i * (N - per) / (runs - 1)) for i in range(runs)]
+    res = {}
+    for K in (128, 300, 512):
+        env = e.addEnvironmentMap(eng.EnvironmentMap(faces), K=K)
+        idx, st = e.envWavelets(env)
+        ref = np.concatenate([O.relight_f64(b, idx, st, px_begin=s, px_end=s + per) for s in starts])
+        sel = np.concatenate([np.arange(s, s + per) for s in starts])
+        row = {}
+        for prec in ("bf16", "fp32"):
+            cfg = eng.RenderConfig(precision=prec)
+            e.TCNNPass_p2(env, 0, cfg)
+            torch.cuda.synchronize()
+            a, bb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            e.TCNNPass_p2(env, 0, cfg)
+            bb.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(bb)
+            got = fr.fbPredictedIndirect[torch.from_numpy(sel).to(dev)][:, :3].double().cpu().numpy()
+            floor = 1e-6 * np.abs(ref).max()
+            rel = np.abs(got - ref) / np.maximum(np.abs(ref), floor)
+            mse = float(np.mean((got - ref) ** 2))
+            row[prec] = {"ms": ms, "evals_per_s": N * K / (ms / 1e3),
+                         "max_rel_err": float(rel.max()), "mean_rel_err": float(rel.mean()),
+                         "psnr_db": 10 * np.log10(np.abs(ref).max() ** 2 / mse) if mse > 0 else float("inf")}
+        row["fp8_e4m3"] = "not built: the tensor-core path runs BF16 operands only"
+        res[f"K{K}"] = row
+    e.close()
+    if rank == 0:
+        print(json.dumps({"metric": "precision sweep at 1920x1080 vs FP64 oracle", "value": res["K300"]["bf16"]["psnr_db"],
+                          "unit": "dB (BF16 PSNR at K=300)", "n_gpus": world, "higher_is_better": True,
+                          "data": "synthetic", "config": {"workload": "relight 1920x1080, K in {128,300,512}",
+                                                          "oracle_pixels_per_K": runs * per}, "sweep": res}),
+              flush=True)
 
 
 # ---------------------------------------------------------------------------- reference arm
