@@ -41,12 +41,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["auto", "bf16", "fp32"], default="auto")
-    ap.add_argument("--workload", choices=["relight1080", "sh1080", "serve", "sweep"], default="relight1080")
+    ap.add_argument("--workload", choices=["relight1080", "sh1080", "haar", "serve", "sweep"], default="relight1080")
     ap.add_argument("--sweep-px", type=int, default=4096, help="pixels checked against the FP64 oracle per K")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=120.0)
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
                     help="requests of the stream also served by the plain FP32 serial baseline")
+    ap.add_argument("--fp8-steps", type=int, default=5, help="timed steps of the FP8 form (0: skip)")
     ap.add_argument("--fp32-steps", type=int, default=2, help="timed steps of the plain FP32 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -166,6 +167,8 @@ def run_ours(args):
 
     if args.workload == "sh1080":
         return run_sh(args, rank, world, local, dev)
+    if args.workload == "haar":
+        return run_haar(args, rank, world, local, dev)
     if args.workload == "serve":
         return run_serve(args, rank, world, local, dev)
     if args.workload == "sweep":
@@ -272,6 +275,24 @@ def run_ours(args):
         ms32 = timed(step32, args.fp32_steps, 1)
         plain = {"value": world * evals / (ms32 / 1e3), "unit": "evals/s", "ms_per_step": ms32}
 
+    # ---- the FP8 (E4M3) form of the same step, scales from a seeded calibration batch
+    fp8 = None
+    if precision == "bf16" and args.fp8_steps > 0:
+        from neural_wavelet_prt_demo_b200 import synth
+        cal = eng.FullFrame.from_gbuffer(synth.make_gbuffer(256, 256, seed=7), dev)
+        e.setFrame(1, cal)
+        e.TCNNPass_p1(1)
+        e.calibrateFP8(env_id, 1)
+        cfg8 = eng.RenderConfig(precision="fp8")
+
+        def step8():
+            e.TCNNPass_p1(0)
+            e.TCNNPass_p2(env_id, 0, cfg8)
+
+        ms8 = timed(step8, args.fp8_steps, 1)
+        fp8 = {"value": world * evals / (ms8 / 1e3), "unit": "evals/s", "ms_per_step": ms8,
+               "calibration": "256x256 G-buffer seed 7, same env map; accuracy in --workload sweep"}
+
     # ---- roofline of the dominant kernel (the fused relight)
     peaks, peak_src = load_peaks()
     flops = desc.flops_per_eval() * evals
@@ -314,7 +335,7 @@ def run_ours(args):
                        "l2": f"inputs {h2d / 1e6:.0f} MB/frame vs 126 MB L2 (no flush)",
                        "parallelism": f"request-dp{world}", "step": "TCNNPass_p1 + TCNNPass_p2"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
-            "clocks": clocks, "plain_fp32": plain,
+            "clocks": clocks, "plain_fp32": plain, "fp8_e4m3": fp8,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -365,6 +386,81 @@ def run_sh(args, rank, world, local, dev):
                           "gpu_launches": args.steps}), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+HAAR_MAPS, HAAR_S, HAAR_K = 1024, 64, 300
+
+
+def run_haar(args, rank, world, local, dev):
+    """Batched Haar transform + top-K: HAAR_MAPS 6x64x64 env maps per launch (302 MB of
+    faces, larger than L2), K=300, plus the latency of a single-map launch."""
+    import torch
+    import torch.distributed as dist
+    from neural_wavelet_prt_demo_b200 import engine as eng, synth
+    from neural_wavelet_prt_demo_b200.sharding import max_over_ranks
+    from oracle import oracle as O
+    g = torch.Generator(device=dev).manual_seed(rank)
+    # log-normal(0, 1.5) radiance, the env-map distribution of the relight workloads
+    faces = torch.exp(1.5 * torch.randn((HAAR_MAPS, 6, HAAR_S, HAAR_S, 3), generator=g, device=dev))
+    for _ in range(args.warmup):
+        eng.haar_topk(faces, HAAR_K)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local)
+    clk.start()
+    a.record()
+    for _ in range(args.steps):
+        idx, st = eng.haar_topk(faces, HAAR_K)
+    b.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = max_over_ranks(a.elapsed_time(b), device=dev) / args.steps
+    one = faces[:1].contiguous()
+    for _ in range(3):
+        eng.haar_topk(one, HAAR_K)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(20):
+        eng.haar_topk(one, HAAR_K)
+    b.record()
+    torch.cuda.synchronize()
+    single_us = a.elapsed_time(b) / 20 * 1e3
+    per_map = 6 * HAAR_S * HAAR_S * 3 * 4 + HAAR_K * 16
+    gbs = HAAR_MAPS * per_map / (ms / 1e3) / 1e9
+    peaks, src = load_peaks()
+    ok = True
+    if rank == 0:
+        # parity spot check on a few maps, then the oracle timed on the host cores
+        sub = faces[:4].cpu().numpy()
+        ridx, rst = O.haar_topk(sub, HAAR_K)
+        ok = bool(np.array_equal(ridx, idx[:4].cpu().numpy()) and
+                  np.array_equal(rst.view(np.uint32), st[:4].cpu().numpy().view(np.uint32)))
+        cpu = None
+        if not args.no_cpu_baseline:
+            host = faces[:64].cpu().numpy()
+            threads = O.max_threads()
+            t0 = time.perf_counter()
+            O.haar_topk(host, HAAR_K, n_threads=threads)
+            dt = time.perf_counter() - t0
+            cpu = {"value": 64 * per_map / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+                   "sample": "64 maps of the same batch, oracle Haar + top-K on all host threads"}
+        print(json.dumps({"metric": "Haar + top-K GB/s (1024 6x64x64 env maps, K=300)", "value": gbs * world,
+                          "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32", "data": "synthetic: log-normal(0,1.5) env maps",
+                          "config": {"workload": f"haar_topk {HAAR_MAPS}x6x{HAAR_S}x{HAAR_S}x3 K={HAAR_K}",
+                                     "l2": "inputs 302 MB vs 126 MB L2 (no flush)"},
+                          "roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                       "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                                       "peak_source": src},
+                          "single_map_us": single_us, "parity_bit_exact_4_maps": ok,
+                          "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": args.steps}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    if not ok:
+        raise SystemExit("haar_topk differs from the oracle")
 
 
 # ---------------------------------------------------------------------------- serving stream
@@ -459,9 +555,11 @@ def run_serve(args, rank, world, local, dev):
 # ---------------------------------------------------------------------------- precision sweep
 
 def run_sweep(args, rank, world, local, dev):
-    """Config-3 precision sweep: the 1080p frame relit at K in {128, 300, 512} in BF16 and in
-    FP32; per K, throughput and max / mean relative error and PSNR against the FP64 oracle of
-    the same network and weights on a pixel sample spread over the frame."""
+    """Config-3 precision sweep: the 1080p frame relit at K in {128, 300, 512} in BF16, FP8
+    (E4M3, per-layer scales) and FP32; per K, throughput and max / mean relative error and
+    PSNR against the FP64 oracle of the same network and weights on a pixel sample spread
+    over the frame.  The FP8 scales come from one seeded calibration batch (a separate
+    256x256 synthetic G-buffer relit with the K=300 env map) and stay fixed for every K."""
     import torch
     from neural_wavelet_prt_demo_b200 import engine as eng
     from oracle import oracle as O
@@ -477,13 +575,20 @@ def run_sweep(args, rank, world, local, dev):
     runs, per = 16, max(1, args.sweep_px // 16)
     starts = [int(i * (N - per) / (runs - 1)) for i in range(runs)]
     res = {}
+    from neural_wavelet_prt_demo_b200 import synth
+    cal = eng.FullFrame.from_gbuffer(synth.make_gbuffer(256, 256, seed=7), dev)
+    e.setFrame(1, cal)
+    e.TCNNPass_p1(1)
+    cal_env = e.addEnvironmentMap(eng.EnvironmentMap(faces), K=300)
+    amax = e.calibrateFP8(cal_env, 1)
+    e.releaseEnvironmentMap(cal_env)
     for K in (128, 300, 512):
         env = e.addEnvironmentMap(eng.EnvironmentMap(faces), K=K)
         idx, st = e.envWavelets(env)
         ref = np.concatenate([O.relight_f64(b, idx, st, px_begin=s, px_end=s + per) for s in starts])
         sel = np.concatenate([np.arange(s, s + per) for s in starts])
         row = {}
-        for prec in ("bf16", "fp32"):
+        for prec in ("bf16", "fp8", "fp32"):
             cfg = eng.RenderConfig(precision=prec)
             e.TCNNPass_p2(env, 0, cfg)
             torch.cuda.synchronize()
@@ -500,14 +605,17 @@ def run_sweep(args, rank, world, local, dev):
             row[prec] = {"ms": ms, "evals_per_s": N * K / (ms / 1e3),
                          "max_rel_err": float(rel.max()), "mean_rel_err": float(rel.mean()),
                          "psnr_db": 10 * np.log10(np.abs(ref).max() ** 2 / mse) if mse > 0 else float("inf")}
-        row["fp8_e4m3"] = "not built: the tensor-core path runs BF16 operands only"
+        row["fp8_e4m3"] = row.pop("fp8")
         res[f"K{K}"] = row
     e.close()
     if rank == 0:
         print(json.dumps({"metric": "precision sweep at 1920x1080 vs FP64 oracle", "value": res["K300"]["bf16"]["psnr_db"],
                           "unit": "dB (BF16 PSNR at K=300)", "n_gpus": world, "higher_is_better": True,
                           "data": "synthetic", "config": {"workload": "relight 1920x1080, K in {128,300,512}",
-                                                          "oracle_pixels_per_K": runs * per}, "sweep": res}),
+                                                          "oracle_pixels_per_K": runs * per,
+                                                          "fp8_calibration": "256x256 G-buffer seed 7, K=300",
+                                                          "fp8_layer_amax": [float(x) for x in amax]},
+                          "sweep": res}),
               flush=True)
 
 

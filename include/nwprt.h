@@ -51,7 +51,9 @@ typedef enum {
 /* Transport MLP arithmetic. */
 typedef enum {
   NWPRT_PREC_FP32 = 0, /* plain FP32 SIMT path: the drop-in, <= 1e-5 rel vs the FP32 reference math */
-  NWPRT_PREC_BF16 = 1  /* tcgen05 tensor cores, BF16 operands, FP32 accumulate */
+  NWPRT_PREC_BF16 = 1, /* tcgen05 tensor cores, BF16 operands, FP32 accumulate */
+  NWPRT_PREC_FP8 = 2   /* tcgen05 tensor cores, E4M3 operands with per-layer scales, FP32 accumulate;
+                          needs nwprt_calibrate_fp8 after the weights are loaded */
 } nwprt_precision;
 
 typedef struct nwprt_ctx nwprt_ctx;
@@ -181,10 +183,24 @@ NWPRT_API nwprt_status nwprt_relight(nwprt_ctx* ctx, int env_id, int frame_id,
 /* Many relights in one device pass (cross-request batching for serving). */
 NWPRT_API nwprt_status nwprt_relight_batch(nwprt_ctx* ctx, const nwprt_request* reqs, int n_reqs,
                                  const nwprt_relight_opts* opts, void* stream);
-/* Pixel-range relights, all in one device pass for NWPRT_PREC_BF16 (one launch per
- * range for NWPRT_PREC_FP32).  Ranges of one frame/output may not overlap within a call. */
+/* Pixel-range relights, all in one device pass for NWPRT_PREC_BF16 / NWPRT_PREC_FP8 (one
+ * launch per range for NWPRT_PREC_FP32).  Ranges of one frame/output may not overlap
+ * within a call. */
 NWPRT_API nwprt_status nwprt_relight_ranges(nwprt_ctx* ctx, const nwprt_range_request* reqs, int n_reqs,
                                             const nwprt_relight_opts* opts, void* stream);
+/* FP8 calibration (no reference counterpart: the reference runs tcnn's FP16 network,
+ * prt_network.h:53-60).  Relights pixels [px_begin, px_end) of a prepared frame (px_end
+ * <= 0: to the end of the frame) with env `env_id` in BF16, records the maximum activation
+ * entering every tensor-core layer, and builds the FP8 weights and per-layer scales from
+ * them.  The scales then stay fixed for every NWPRT_PREC_FP8 relight until the next
+ * calibration or weight load, so a result does not depend on what it is batched with.
+ * Blocks on `stream`, then on the device before it replaces a previous FP8 blob. */
+NWPRT_API nwprt_status nwprt_calibrate_fp8(nwprt_ctx* ctx, int env_id, int frame_id, int64_t px_begin,
+                                           int64_t px_end, void* stream);
+/* The calibrated maxima: one per tensor-core layer input, then the input of the 3-wide
+ * output layer.  Writes min(capacity, n) values and sets *n_values = n. */
+NWPRT_API nwprt_status nwprt_get_fp8_calibration(const nwprt_ctx* ctx, float* amax, int capacity,
+                                                 int* n_values);
 /* Blocks until all work the context issued has finished -- RenderEngine::TCNNSync
  * (tinycudann/tcnn.cu:154-158). */
 NWPRT_API nwprt_status nwprt_sync(nwprt_ctx* ctx);

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libnwprt.so")
 
 OK, INVALID_ARG, OOM, CUDA_ERROR, TIMEOUT, NOT_READY, IO_ERROR, UNSUPPORTED = range(8)
-PREC_FP32, PREC_BF16 = 0, 1
+PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
 MAX_FRAMES = 16
 
 # Every symbol include/nwprt.h declares (checked by the CPU test suite).
@@ -21,7 +21,8 @@ EXPORTS = (
     "nwprt_abi_version", "nwprt_status_string", "nwprt_last_error", "nwprt_create", "nwprt_destroy",
     "nwprt_get_network_info", "nwprt_load_weights", "nwprt_load_weights_dir", "nwprt_ready",
     "nwprt_env_from_faces", "nwprt_env_from_wavelets", "nwprt_env_get_wavelets", "nwprt_env_release",
-    "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_relight_ranges", "nwprt_sync",
+    "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_relight_ranges",
+    "nwprt_calibrate_fp8", "nwprt_get_fp8_calibration", "nwprt_sync",
     "nwprt_haar_topk", "nwprt_env_rotate",
     "nwprt_sh_project_workspace_size", "nwprt_sh_project", "nwprt_sh_project_static", "nwprt_sh_dot",
 )
@@ -97,6 +98,8 @@ def lib():
         "nwprt_relight": (_st, [_vp, _i, _i, C.POINTER(RelightOpts), _vp, _vp, _vp]),
         "nwprt_relight_batch": (_st, [_vp, C.POINTER(Request), _i, C.POINTER(RelightOpts), _vp]),
         "nwprt_relight_ranges": (_st, [_vp, C.POINTER(RangeRequest), _i, C.POINTER(RelightOpts), _vp]),
+        "nwprt_calibrate_fp8": (_st, [_vp, _i, _i, C.c_int64, C.c_int64, _vp]),
+        "nwprt_get_fp8_calibration": (_st, [_vp, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
         "nwprt_sync": (_st, [_vp]),
         "nwprt_env_rotate": (_st, [_vp, _i, _vp, _vp, _vp]),
         "nwprt_haar_topk": (_st, [_vp, _i, _i, _i, _vp, _vp, _vp]),

@@ -83,6 +83,13 @@ struct nwprt_ctx {
   uint16_t* d_tc_w = nullptr;
   bool tc_supported = false;
   std::string tc_why;
+  // FP8: host copies of the MLP weights (the blob is rebuilt at every calibration), the
+  // calibrated per-layer activation maxima and the plan/blob built from them
+  std::vector<float> h_op, h_cn;
+  uint8_t* d_tc_w8 = nullptr;
+  TcPlan fp8_plan{};
+  bool fp8_ready = false;
+  std::vector<float> fp8_amax;
   std::vector<EnvEntry> envs;
   Frame frames[NWPRT_MAX_FRAMES];
   uint32_t* d_err = nullptr;
@@ -98,6 +105,7 @@ struct nwprt_ctx {
     dev_free(d_emb);
     dev_free(d_w32);
     dev_free(d_tc_w);
+    dev_free(d_tc_w8);
     dev_free(d_err);
     dev_free(d_stage);
     dev_free(d_jobs);
@@ -307,8 +315,12 @@ nwprt_status nwprt_load_weights(nwprt_ctx* ctx, const nwprt_weights* w) {
     dev_free(ctx->d_emb);
     dev_free(ctx->d_w32);
     dev_free(ctx->d_tc_w);
+    dev_free(ctx->d_tc_w8);
     ctx->d_hash = ctx->d_emb = ctx->d_w32 = nullptr;
     ctx->d_tc_w = nullptr;
+    ctx->d_tc_w8 = nullptr;
+    ctx->fp8_ready = false;
+    ctx->fp8_amax.clear();
     ctx->weights_loaded = false;
     ctx->d_hash = dev_alloc<float>(w->n_hash_params);
     NWPRT_CUDA(cudaMemcpy(ctx->d_hash, w->hash_params, w->n_hash_params * 4, cudaMemcpyHostToDevice));
@@ -321,6 +333,8 @@ nwprt_status nwprt_load_weights(nwprt_ctx* ctx, const nwprt_weights* w) {
     ctx->d_w32 = dev_alloc<float>(op_t.size() + cn_t.size());
     NWPRT_CUDA(cudaMemcpy(ctx->d_w32, op_t.data(), op_t.size() * 4, cudaMemcpyHostToDevice));
     NWPRT_CUDA(cudaMemcpy(ctx->d_w32 + op_t.size(), cn_t.data(), cn_t.size() * 4, cudaMemcpyHostToDevice));
+    ctx->h_op.assign(w->out_prd, w->out_prd + w->n_out_prd);
+    ctx->h_cn.assign(w->cmp_net, w->cmp_net + w->n_cmp_net);
     if (ctx->tc_supported) {
       std::vector<uint16_t> tw;
       pack_tc_weights(d, w->out_prd, w->cmp_net, &tw);
@@ -513,9 +527,11 @@ static void relight_one(nwprt_ctx* ctx, RangeReq r, const nwprt_relight_opts& o,
 }
 
 static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, const nwprt_relight_opts& o,
-                            cudaStream_t st) {
+                            int mode, uint32_t* amax, cudaStream_t st) {
   need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
   need(ctx->tc_supported, NWPRT_UNSUPPORTED, ctx->tc_why.c_str());
+  if (mode == kTcFp8)
+    need(ctx->fp8_ready, NWPRT_NOT_READY, "FP8 scales are not calibrated (call nwprt_calibrate_fp8 first)");
   std::vector<TcJob> jobs;
   jobs.reserve(n_reqs);
   for (int i = 0; i < n_reqs; ++i) {
@@ -536,14 +552,20 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
     ctx->d_jobs = dev_alloc<TcJob>(jobs.size());
     ctx->jobs_cap = (int)jobs.size();
   }
-  launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, jobs.data(), (int)jobs.size(),
-                    ctx->d_jobs, o.kahan, o.clamp_terms, ctx->d_err, st);
+  if (mode == kTcFp8)
+    launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w8, &ctx->fp8_plan, mode, jobs.data(),
+                      (int)jobs.size(), ctx->d_jobs, o.kahan, o.clamp_terms, nullptr, ctx->d_err, st);
+  else
+    launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, nullptr, mode, jobs.data(), (int)jobs.size(),
+                      ctx->d_jobs, o.kahan, o.clamp_terms, amax, ctx->d_err, st);
 }
 
 static void relight_ranges(nwprt_ctx* ctx, const std::vector<RangeReq>& reqs, const nwprt_relight_opts& o,
                            cudaStream_t st) {
   if (o.precision == NWPRT_PREC_BF16) {
-    relight_many_tc(ctx, reqs.data(), (int)reqs.size(), o, st);
+    relight_many_tc(ctx, reqs.data(), (int)reqs.size(), o, kTcBf16, nullptr, st);
+  } else if (o.precision == NWPRT_PREC_FP8) {
+    relight_many_tc(ctx, reqs.data(), (int)reqs.size(), o, kTcFp8, nullptr, st);
   } else {
     for (const RangeReq& r : reqs) relight_one(ctx, r, o, st);
   }
@@ -582,6 +604,77 @@ nwprt_status nwprt_relight_ranges(nwprt_ctx* ctx, const nwprt_range_request* req
       v.push_back(RangeReq{reqs[i].env_id, reqs[i].frame_id, reqs[i].indirect, reqs[i].with_direct,
                            reqs[i].px_begin, reqs[i].px_end});
     relight_ranges(ctx, v, o, (cudaStream_t)stream);
+  });
+}
+
+nwprt_status nwprt_calibrate_fp8(nwprt_ctx* ctx, int env_id, int frame_id, int64_t px_begin, int64_t px_end,
+                                void* stream) {
+  return guarded(ctx, [&] {
+    need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
+    need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
+    std::string why;
+    need(relight_tc_fp8_supported(ctx->dims, &why), NWPRT_UNSUPPORTED, why.c_str());
+    cudaStream_t st = (cudaStream_t)stream;
+    RangeReq r{env_id, frame_id, nullptr, nullptr, px_begin, px_end};
+    {
+      // the range is checked before anything is allocated
+      need(frame_id >= 0 && frame_id < NWPRT_MAX_FRAMES, NWPRT_INVALID_ARG, "frame id out of range");
+      Frame& f = ctx->frames[frame_id];
+      need(f.prepared, NWPRT_NOT_READY, "frame was not prepared (call nwprt_prepare first)");
+      const int64_t n = (int64_t)f.width * f.height;
+      if (r.px_end <= 0) r.px_end = n;
+      need(r.px_begin >= 0 && r.px_begin < r.px_end && r.px_end <= n, NWPRT_INVALID_ARG,
+           "calibration range must be a non-empty pixel range inside the frame");
+    }
+    const int n_layers = tc_layer_count(ctx->dims);
+    const int64_t n_px = r.px_end - r.px_begin;
+    // scratch outputs: the calibration pass is a full BF16 relight of the range
+    float* out = dev_alloc<float>((size_t)n_px * 8);
+    uint32_t* amax = nullptr;
+    try {
+      amax = dev_alloc<uint32_t>(n_layers + 1);
+      NWPRT_CUDA(cudaMemsetAsync(amax, 0, (n_layers + 1) * 4, st));
+      // outputs are indexed by absolute pixel: offset the scratch so the range lands in it
+      r.indirect = out - r.px_begin * 4;
+      r.with_direct = out + n_px * 4 - r.px_begin * 4;
+      relight_many_tc(ctx, &r, 1, default_opts(), kTcCalibrate, amax, st);
+      std::vector<uint32_t> bits(n_layers + 1);
+      NWPRT_CUDA(cudaMemcpyAsync(bits.data(), amax, bits.size() * 4, cudaMemcpyDeviceToHost, st));
+      NWPRT_CUDA(cudaStreamSynchronize(st));
+      uint32_t err = 0;
+      NWPRT_CUDA(cudaMemcpy(&err, ctx->d_err, 4, cudaMemcpyDeviceToHost));
+      need(err == kDevOk, NWPRT_TIMEOUT, "the calibration pass reported a device error");
+      std::vector<float> am(n_layers + 1);
+      std::memcpy(am.data(), bits.data(), am.size() * 4);
+      std::vector<uint8_t> blob;
+      TcPlan plan = pack_tc_weights_fp8(ctx->dims, ctx->h_op.data(), ctx->h_cn.data(), am.data(), &blob);
+      // no launch may still read the previous blob
+      NWPRT_CUDA(cudaDeviceSynchronize());
+      dev_free(ctx->d_tc_w8);
+      ctx->d_tc_w8 = nullptr;
+      ctx->fp8_ready = false;
+      ctx->d_tc_w8 = dev_alloc<uint8_t>(blob.size());
+      NWPRT_CUDA(cudaMemcpy(ctx->d_tc_w8, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+      ctx->fp8_plan = plan;
+      ctx->fp8_amax = am;
+      ctx->fp8_ready = true;
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      dev_free(out);
+      dev_free(amax);
+      throw;
+    }
+    dev_free(out);
+    dev_free(amax);
+  });
+}
+
+nwprt_status nwprt_get_fp8_calibration(const nwprt_ctx* ctx, float* amax, int capacity, int* n_values) {
+  return guarded(ctx, [&] {
+    need(ctx && n_values && (amax || capacity == 0) && capacity >= 0, NWPRT_INVALID_ARG, "bad argument");
+    need(ctx->fp8_ready, NWPRT_NOT_READY, "FP8 scales are not calibrated");
+    *n_values = (int)ctx->fp8_amax.size();
+    for (int i = 0; i < capacity && i < *n_values; ++i) amax[i] = ctx->fp8_amax[i];
   });
 }
 

@@ -145,10 +145,37 @@ void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWei
 void pack_fp32_weights(const NetDims& d, const float* op, const float* cn,
                        std::vector<float>* op_t, std::vector<float>* cn_t);
 
-// relight_tc.cu (tcgen05 BF16 path)
+// relight_tc.cu (tcgen05 path: BF16 operands, or FP8 e4m3 with per-layer scales)
+constexpr int kMaxTcLayers = 12;
+// One tensor-core layer of the per-wavelet MLP chain (B operand offsets inside the weight blob).
+struct TcLayer {
+  uint32_t b_off;  // byte offset of B (N x K, canonical K-major) in the weight blob
+  uint32_t b_sbo;  // B stride between 8-row groups (= K * element bytes * 8)
+  int k;           // reduction length (multiple of 16 for BF16, of 32 for FP8)
+  int n;           // output width: 32 or 64
+  int relu;
+  int aux;         // also accumulate aux (K=16, BF16) x aux block of B at aux_off
+  uint32_t aux_off;
+  int fin;         // the epilogue forms T_k = V_last relu(h) from this layer's output
+  float scale;     // FP8: factor applied to the accumulator before the e4m3 conversion (1 = none)
+};
+struct TcPlan {
+  TcLayer layers[kMaxTcLayers];
+  int n_layers = 0;
+  uint32_t vlast_off = 0;   // byte offset of V_last (FP32 [3][64]) in the blob
+  uint32_t blob_bytes = 0;
+  float cp_scale = 1.f;     // FP8: scale of the first layer's operand hash(p) * E_k
+};
+enum TcMode { kTcBf16 = 0, kTcCalibrate = 1, kTcFp8 = 2 };
 bool relight_tc_supported(const NetDims& d, std::string* why);
+bool relight_tc_fp8_supported(const NetDims& d, std::string* why);
 size_t tc_weight_bytes(const NetDims& d);
 void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);
+// FP8 weight blob from calibrated activation maxima amax[0..n_layers) (the input of every
+// tensor-core layer); returns the plan whose scales the kernel applies.
+TcPlan pack_tc_weights_fp8(const NetDims& d, const float* op, const float* cn, const float* amax,
+                           std::vector<uint8_t>* out);
+int tc_layer_count(const NetDims& d);
 size_t relight_tc_smem_bytes(const NetDims& d);
 struct TcJob {
   const float* packed;    // [n_px][16]
@@ -163,9 +190,12 @@ struct TcJob {
   long long tile_begin;   // first 128-pixel tile of this job in the launch (set by the launcher)
   int64_t px_begin;       // start of the pixel range
 };
-void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash,
-                       const uint16_t* tc_weights_dev, const TcJob* jobs, int n_jobs,
-                       TcJob* jobs_dev, int kahan, int clamp, uint32_t* err, cudaStream_t st);
+// mode kTcBf16 / kTcCalibrate use the BF16 blob (plan == nullptr: derived from d);
+// kTcCalibrate also records per-layer activation maxima into amax (uint bits of floats);
+// kTcFp8 uses the FP8 blob and its plan.
+void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
+                       const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, TcJob* jobs_dev, int kahan,
+                       int clamp, uint32_t* amax, uint32_t* err, cudaStream_t st);
 
 }  // namespace nwprt
 

@@ -38,7 +38,6 @@ constexpr int kNWG = 4;                    // warpgroups per CTA, one tile each
 constexpr int kThreads = 128 * kNWG;
 constexpr int kTile = 128;                 // pixels per tile (MMA M)
 constexpr int kAuxBytes = kTile * 16 * 2;  // 128 x 16 bf16 aux operand
-constexpr int kMaxTcLayers = 12;
 constexpr int kTmemCols = 512;
 constexpr int kTileCols = 128;             // TMEM columns per tile
 constexpr int kAcol = 0;                   // A operand columns [0, 32)
@@ -46,17 +45,6 @@ constexpr int kDcol = 64;                  // accumulator columns [64, 128)
 constexpr int kVlastFloats = 3 * 64;
 constexpr uint64_t kWaitNs = 2000000000ull;
 static_assert(kNWG * kTileCols <= kTmemCols, "TMEM budget");
-
-struct TcLayer {
-  uint32_t b_off;  // byte offset of B (N x K, canonical K-major) in the weight blob
-  uint32_t b_sbo;  // B stride between 8-row groups (= K * 16 bytes)
-  int k;           // reduction length (multiple of 16)
-  int n;           // output width: 32 or 64
-  int relu;
-  int aux;         // also accumulate aux (K=16) x aux block of B at aux_off
-  uint32_t aux_off;
-  int fin;         // the epilogue forms T_k = V_last relu(h) from this layer's output
-};
 
 struct TcParams {
   HashLevels hl;
@@ -71,6 +59,8 @@ struct TcParams {
   int n_jobs;
   long long total_tiles;
   int kahan, clamp;
+  float cp_scale;   // FP8: scale of the first layer's operand
+  uint32_t* amax;   // calibration: per-layer activation maxima (float bits)
   uint32_t* err;
 };
 
@@ -129,6 +119,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
+// kind::f8f6f4 instruction descriptor: D=F32, A=B=E4M3 (format code 0), both K-major, M=128.
+__host__ __device__ constexpr uint32_t idesc_e4m3(int n) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
 
 // D[tmem] (+)= A[tmem] * B[smem]^T
 __device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
@@ -137,6 +131,17 @@ __device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// D[tmem] (+)= A[tmem] * B[smem]^T with E4M3 operands (K = 32 per instruction)
+__device__ __forceinline__ void mma_ts_e4m3(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
       "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate)
       : "memory");
 }
@@ -214,6 +219,20 @@ __device__ __forceinline__ uint32_t pack_bf16_relu(float lo, float hi) {
   asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
+// Four FP32 values -> four E4M3 bytes (round to nearest even, saturated to +-448), x0 in
+// the lowest byte: the K order of an 8-bit operand in one 32-bit TMEM column.
+template <bool RELU>
+__device__ __forceinline__ uint32_t pack_e4m3x4(float x0, float x1, float x2, float x3) {
+  unsigned short lo, hi;
+  if (RELU) {
+    asm("cvt.rn.satfinite.relu.e4m3x2.f32 %0, %1, %2;" : "=h"(lo) : "f"(x1), "f"(x0));
+    asm("cvt.rn.satfinite.relu.e4m3x2.f32 %0, %1, %2;" : "=h"(hi) : "f"(x3), "f"(x2));
+  } else {
+    asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(lo) : "f"(x1), "f"(x0));
+    asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(hi) : "f"(x3), "f"(x2));
+  }
+  return (uint32_t)lo | ((uint32_t)hi << 16);
+}
 __device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 
@@ -226,6 +245,41 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t
 // 8-row groups are `sbo` bytes apart.
 __device__ __forceinline__ uint32_t core_off(int row, int chunk, uint32_t sbo) {
   return (uint32_t)(row >> 3) * sbo + (uint32_t)chunk * 128u + (uint32_t)(row & 7) * 16u;
+}
+
+// 32 FP32 TMEM values (times `scale`, a uniform per-layer value) -> 8 E4M3 quads.
+template <bool RELU>
+__device__ __forceinline__ void pack32_e4m3(const uint32_t (&v)[32], float scale, uint32_t* out) {
+  if (scale == 1.f) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      out[j] = pack_e4m3x4<RELU>(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                 __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float x[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) x[i] = __fmul_rn(__uint_as_float(v[4 * j + i]), scale);
+      out[j] = pack_e4m3x4<RELU>(x[0], x[1], x[2], x[3]);
+    }
+  }
+}
+
+// Largest value this warp passes to the next layer (ReLU'd, or |v| for a linear layer),
+// folded into the layer's calibration maximum.  Non-negative floats order like their bits.
+__device__ __forceinline__ uint32_t amax32(const uint32_t (&v)[32], bool relu) {
+  float m = 0.f;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const float x = __uint_as_float(v[i]);
+    m = fmaxf(m, relu ? x : fabsf(x));
+  }
+  return __float_as_uint(m);
+}
+__device__ __forceinline__ void record_amax(uint32_t* slot, uint32_t bits) {
+  bits = __reduce_max_sync(0xffffffffu, bits);
+  if ((threadIdx.x & 31) == 0) atomicMax(slot, bits);
 }
 
 // 32 FP32 TMEM values -> 16 BF16 pairs.
@@ -297,23 +351,48 @@ __device__ __forceinline__ void hash_encode_bf16(const HashLevels& hl, const flo
   }
 }
 
-// First-layer operand of wavelet k (hash(p) * E_k, rounded once to BF16) -> TMEM A columns.
-template <int DMAX>
+// First-layer operand of wavelet k, hash(p) * E_k -> TMEM A columns: rounded once to BF16,
+// or (FP8) scaled by cp_scale and rounded to E4M3, zero-padded to K = 32.  Calibration
+// records max |hash(p) * E_k| in amax[0].
+template <int DMAX, int MODE>
 __device__ __forceinline__ void store_cp(const uint32_t (&enc)[DMAX / 2], const float* __restrict__ ek,
-                                         uint32_t a_taddr) {
-  uint32_t cp[DMAX / 2];
+                                         uint32_t a_taddr, float cp_scale, uint32_t* amax) {
+  float x[DMAX];
 #pragma unroll
   for (int c = 0; c < DMAX / 8; ++c) {
     const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
     const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
     const uint32_t h0 = enc[c * 4 + 0], h1 = enc[c * 4 + 1], h2 = enc[c * 4 + 2], h3 = enc[c * 4 + 3];
-    cp[c * 4 + 0] = pack_bf16(__fmul_rn(bf16_lo(h0), e0.x), __fmul_rn(bf16_hi(h0), e0.y));
-    cp[c * 4 + 1] = pack_bf16(__fmul_rn(bf16_lo(h1), e0.z), __fmul_rn(bf16_hi(h1), e0.w));
-    cp[c * 4 + 2] = pack_bf16(__fmul_rn(bf16_lo(h2), e1.x), __fmul_rn(bf16_hi(h2), e1.y));
-    cp[c * 4 + 3] = pack_bf16(__fmul_rn(bf16_lo(h3), e1.z), __fmul_rn(bf16_hi(h3), e1.w));
+    x[c * 8 + 0] = __fmul_rn(bf16_lo(h0), e0.x);
+    x[c * 8 + 1] = __fmul_rn(bf16_hi(h0), e0.y);
+    x[c * 8 + 2] = __fmul_rn(bf16_lo(h1), e0.z);
+    x[c * 8 + 3] = __fmul_rn(bf16_hi(h1), e0.w);
+    x[c * 8 + 4] = __fmul_rn(bf16_lo(h2), e1.x);
+    x[c * 8 + 5] = __fmul_rn(bf16_hi(h2), e1.y);
+    x[c * 8 + 6] = __fmul_rn(bf16_lo(h3), e1.z);
+    x[c * 8 + 7] = __fmul_rn(bf16_hi(h3), e1.w);
   }
-  if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
-  else tmem_st8(a_taddr, cp);
+  if constexpr (MODE == kTcFp8) {
+    uint32_t cp[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      cp[i] = i < DMAX / 4 ? pack_e4m3x4<false>(__fmul_rn(x[4 * i], cp_scale), __fmul_rn(x[4 * i + 1], cp_scale),
+                                                __fmul_rn(x[4 * i + 2], cp_scale), __fmul_rn(x[4 * i + 3], cp_scale))
+                           : 0u;
+    tmem_st8(a_taddr, cp);
+  } else {
+    uint32_t cp[DMAX / 2];
+#pragma unroll
+    for (int i = 0; i < DMAX / 2; ++i) cp[i] = pack_bf16(x[2 * i], x[2 * i + 1]);
+    if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
+    else tmem_st8(a_taddr, cp);
+    if constexpr (MODE == kTcCalibrate) {
+      float m = 0.f;
+#pragma unroll
+      for (int i = 0; i < DMAX; ++i) m = fmaxf(m, fabsf(x[i]));
+      record_amax(amax, __float_as_uint(m));
+    }
+  }
 }
 
 __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long tile) {
@@ -333,23 +412,35 @@ struct __align__(8) TcBarriers {
 };
 
 // Issues layer L of warpgroup g's tile: A from TMEM (and the aux block from shared memory).
+// A K step covers 32 bytes of a row in both precisions (16 BF16 or 32 E4M3 values): 8 TMEM
+// columns of A and two 128-byte core-matrix columns of B.  The aux block stays BF16 in both;
+// its MMA accumulates into the same FP32 accumulator.
+template <int MODE>
 __device__ __forceinline__ void issue_layer(const TcLayer& L, uint32_t wbase, uint32_t a_tmem, uint32_t aux_base,
                                             uint32_t d_tmem, uint64_t* bar) {
   tc_fence_after();
-  const uint32_t id = idesc_bf16(L.n);
-  for (int s = 0; s < L.k / 16; ++s) {
-    const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
-    mma_ts(d_tmem, a_tmem + (uint32_t)s * 8u, bd, id, s > 0 ? 1u : 0u);
+  if constexpr (MODE == kTcFp8) {
+    const uint32_t id = idesc_e4m3(L.n);
+    for (int s = 0; s < L.k / 32; ++s) {
+      const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
+      mma_ts_e4m3(d_tmem, a_tmem + (uint32_t)s * 8u, bd, id, s > 0 ? 1u : 0u);
+    }
+  } else {
+    const uint32_t id = idesc_bf16(L.n);
+    for (int s = 0; s < L.k / 16; ++s) {
+      const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
+      mma_ts(d_tmem, a_tmem + (uint32_t)s * 8u, bd, id, s > 0 ? 1u : 0u);
+    }
   }
   if (L.aux) {
     const uint64_t ad = smem_desc(aux_base, 128u, 256u);
     const uint64_t bd = smem_desc(wbase + L.aux_off, 128u, 256u);
-    mma_ss(d_tmem, ad, bd, id, 1u);
+    mma_ss(d_tmem, ad, bd, idesc_bf16(L.n), 1u);
   }
   mma_commit(bar);
 }
 
-template <int DMAX>
+template <int DMAX, int MODE>
 __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_constant__ TcParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;                                       // weight blob (+ V_last)
@@ -421,14 +512,14 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
       st_shared_v4(aux_row, 0, 0, 0, 0);
       st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
     }
-    store_cp<DMAX>(enc, J.emb_k, a_taddr);
+    store_cp<DMAX, MODE>(enc, J.emb_k, a_taddr, p.cp_scale, p.amax);
     tmem_wait_st();
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     // hand the first layer to the tensor core
     tc_fence_before();
     fence_proxy_async_smem();
     ok = wg_barrier_and(g, ok);
-    if (ok && leader) issue_layer(p.layers[0], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+    if (ok && leader) issue_layer<MODE>(p.layers[0], wbase, a_tmem, aux_base, d_tmem, acc_bar);
     for (int k = 0; k < K && ok; ++k) {
       for (int l = 0; l < p.n_layers; ++l) {
         const TcLayer& L = p.layers[l];
@@ -437,29 +528,52 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         if (waited) {
           tc_fence_after();
           uint32_t v[32];
-          if (!L.fin) {
-            uint32_t a[32];
+          if (!L.fin && MODE == kTcFp8) {
+            uint32_t a[16];
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
+            if (L.relu) pack32_e4m3<true>(v, L.scale, a);
+            else pack32_e4m3<false>(v, L.scale, a);
+            if (L.n > 32) {
+              tmem_ld32(d_taddr + 32u, v);
+              tmem_wait_ld();
+              if (L.relu) pack32_e4m3<true>(v, L.scale, a + 8);
+              else pack32_e4m3<false>(v, L.scale, a + 8);
+              tmem_st16(a_taddr, a);
+            } else {
+              tmem_st8(a_taddr, a);
+            }
+            tmem_wait_st();
+          } else if (!L.fin) {
+            uint32_t a[32];
+            uint32_t m = 0;
+            tmem_ld32(d_taddr, v);
+            tmem_wait_ld();
+            if constexpr (MODE == kTcCalibrate) m = amax32(v, L.relu);
             if (L.relu) pack32<true>(v, a);
             else pack32<false>(v, a);
             if (L.n > 32) {
               tmem_ld32(d_taddr + 32u, v);
               tmem_wait_ld();
+              if constexpr (MODE == kTcCalibrate) m = max(m, amax32(v, L.relu));
               if (L.relu) pack32<true>(v, a + 16);
               else pack32<false>(v, a + 16);
               tmem_st32(a_taddr, a);
             } else {
               tmem_st16(a_taddr, a);
             }
+            if constexpr (MODE == kTcCalibrate) record_amax(p.amax + l + 1, m);
             tmem_wait_st();
           } else {
             float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+            uint32_t m = 0;
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
+            if constexpr (MODE == kTcCalibrate) m = amax32(v, true);
             final_dot32(v, sV, 0, t0, t1, t2);
             tmem_ld32(d_taddr + 32u, v);
             tmem_wait_ld();
+            if constexpr (MODE == kTcCalibrate) record_amax(p.amax + p.n_layers, max(m, amax32(v, true)));
             final_dot32(v, sV, 32, t0, t1, t2);
             const float* Lk = J.strength + (size_t)k * 3;
             float u0 = __fmul_rn(__ldg(Lk + 0), t0);
@@ -475,7 +589,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
               s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
             }
             if (k + 1 < K) {
-              store_cp<DMAX>(enc, J.emb_k + (size_t)(k + 1) * p.enc_dims, a_taddr);
+              store_cp<DMAX, MODE>(enc, J.emb_k + (size_t)(k + 1) * p.enc_dims, a_taddr, p.cp_scale, p.amax);
               tmem_wait_st();
             }
           }
@@ -486,7 +600,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
         if (!ok) break;
-        if (leader) issue_layer(p.layers[nl], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+        if (leader) issue_layer<MODE>(p.layers[nl], wbase, a_tmem, aux_base, d_tmem, acc_bar);
       }
     }
     if (valid && ok) {
@@ -521,30 +635,141 @@ uint16_t to_bf16(float f) {
   return (uint16_t)(u >> 16);
 }
 
-int pad16(int x) { return (x + 15) & ~15; }
+// FP32 -> E4M3 (1 sign, 4 exponent bits with bias 7, 3 mantissa bits; no infinities; max
+// finite 448), round to nearest even, saturated to +-448 like cvt.rn.satfinite.
+uint8_t to_e4m3(float f) {
+  if (std::isnan(f)) return 0x7f;
+  const uint8_t sign = std::signbit(f) ? 0x80 : 0x00;
+  const double a = std::fabs((double)f);
+  if (a >= 464.0) return sign | 0x7e;  // 464 = halfway between 448 and the next step
+  if (a < std::ldexp(1.0, -6)) {       // subnormal: multiples of 2^-9
+    const double q = std::nearbyint(a * 512.0);
+    return sign | (uint8_t)q;          // q == 8 is the smallest normal, code 0x08
+  }
+  int e;
+  const double m = std::frexp(a, &e);  // a = m * 2^e, m in [0.5, 1)
+  double q = std::nearbyint((m * 2.0 - 1.0) * 8.0);
+  int E = e - 1;
+  if (q >= 8.0) {
+    q = 0.0;
+    ++E;
+  }
+  if (E > 8 || (E == 8 && q > 6.0)) return sign | 0x7e;
+  return sign | (uint8_t)(((E + 7) << 3) | (int)q);
+}
 
-// Writes the N x K (row-major [out][in]) block src[:, col0:col0+kc] as a canonical
-// K-major tile of np x kp BF16 (zero padded) at byte offset `off` of the blob.
-void put_b(std::vector<uint16_t>* blob, size_t off, const float* src, int n, int k_total, int col0, int kc,
-           int np, int kp) {
-  const size_t need = off / 2 + (size_t)np * kp;
+int pad16(int x) { return (x + 15) & ~15; }
+int pad32(int x) { return (x + 31) & ~31; }
+
+// Writes the N x K (row-major [out][in]) block src[:, col0:col0+kc] * scale as a canonical
+// K-major tile of np x kp elements (zero padded) of `eb` bytes each at byte offset `off`.
+// Core matrices are 8 rows x 16 bytes; K-adjacent ones are 128 bytes apart, 8-row groups
+// kp * eb * 8 bytes apart.
+void put_b(std::vector<uint8_t>* blob, size_t off, const float* src, int n, int k_total, int col0, int kc,
+           int np, int kp, int eb, float scale) {
+  const size_t need = off + (size_t)np * kp * eb;
   if (blob->size() < need) blob->resize(need, 0);
-  const uint32_t sbo = (uint32_t)kp * 16u;
+  const size_t sbo = (size_t)kp * eb * 8;
   for (int r = 0; r < np; ++r)
     for (int c = 0; c < kp; ++c) {
-      const float v = (r < n && c < kc) ? src[(size_t)r * k_total + col0 + c] : 0.f;
-      const size_t byte = off + (size_t)(r >> 3) * sbo + (size_t)(c >> 3) * 128 + (size_t)(r & 7) * 16 +
-                          (size_t)(c & 7) * 2;
-      (*blob)[byte / 2] = to_bf16(v);
+      const float v = (r < n && c < kc) ? src[(size_t)r * k_total + col0 + c] * scale : 0.f;
+      const size_t cb = (size_t)c * eb;  // byte column within the row
+      const size_t byte = off + (size_t)(r >> 3) * sbo + (cb >> 4) * 128 + (size_t)(r & 7) * 16 + (cb & 15);
+      if (eb == 2) {
+        const uint16_t h = to_bf16(v);
+        std::memcpy(blob->data() + byte, &h, 2);
+      } else {
+        (*blob)[byte] = to_e4m3(v);
+      }
     }
 }
 
-struct Plan {
-  TcLayer layers[kMaxTcLayers];
-  int n_layers = 0;
-  uint32_t vlast_off = 0;
-  std::vector<uint16_t> blob;
+// Layer table of the tensor-core chain: out_prd layers, then cmp_net's hidden layers (the
+// first one with the aux block), the last one marked fin.  Returns for each layer the
+// weight matrix, its [out][in] shape and the column range used.
+struct LayerSrc {
+  const float* w;
+  int n, k_total, col0, kc;
+  bool relu, aux;
 };
+std::vector<LayerSrc> layer_sources(const NetDims& d, const float* op, const float* cn) {
+  std::vector<LayerSrc> v;
+  const float* w = op;
+  for (int i = 0; i < d.op_nl; ++i) {
+    v.push_back({w, d.op_outs[i], d.op_in[i], 0, d.op_in[i], i + 1 < d.op_nl, false});
+    if (w) w += (size_t)d.op_in[i] * d.op_outs[i];
+  }
+  w = cn;
+  for (int i = 0; i + 1 < d.cn_nl; ++i) {
+    v.push_back({w, d.cn_outs[i], d.cn_in[i], 0, i == 0 ? d.op_out : d.cn_in[i], true, i == 0});
+    if (w) w += (size_t)d.cn_in[i] * d.cn_outs[i];
+  }
+  return v;
+}
+const float* vlast_src(const NetDims& d, const float* cn) {
+  if (!cn) return nullptr;
+  const float* w = cn;
+  for (int i = 0; i + 1 < d.cn_nl; ++i) w += (size_t)d.cn_in[i] * d.cn_outs[i];
+  return w;
+}
+
+// Builds the blob for one precision.  eb = 2: BF16, every scale 1.  eb = 1: E4M3 with
+// layer scales g[l] (B = W * g[l]), aux scales (the aux block stays BF16, times dscale of
+// its layer) and V_last divided by the fin layer's accumulator scale.
+TcPlan make_plan(const NetDims& d, const float* op, const float* cn, int eb, const std::vector<float>& g,
+                 const std::vector<float>& dscale, std::vector<uint8_t>* blob) {
+  TcPlan P;
+  size_t off = 0;
+  const bool fill = op && cn;
+  const std::vector<LayerSrc> src = layer_sources(d, op, cn);
+  for (size_t li = 0; li < src.size(); ++li) {
+    const LayerSrc& ls = src[li];
+    TcLayer L{};
+    const int np = pad16(ls.n), kp = eb == 2 ? pad16(ls.kc) : pad32(ls.kc);
+    L.b_off = (uint32_t)off;
+    L.b_sbo = (uint32_t)(kp * eb * 8);
+    L.k = kp;
+    L.n = np;
+    L.relu = ls.relu;
+    L.scale = 1.f;
+    if (fill) put_b(blob, off, ls.w, ls.n, ls.k_total, ls.col0, ls.kc, np, kp, eb, eb == 2 ? 1.f : g[li]);
+    off += (size_t)np * kp * eb;
+    off = (off + 127) & ~size_t(127);
+    if (ls.aux) {
+      // aux block: columns [op_out, op_out + 16) of cmp_net's first layer, BF16
+      L.aux = 1;
+      L.aux_off = (uint32_t)off;
+      if (fill) put_b(blob, off, ls.w, ls.n, ls.k_total, d.op_out, 16, np, 16, 2, eb == 2 ? 1.f : dscale[li]);
+      off += (size_t)np * 16 * 2;
+      off = (off + 127) & ~size_t(127);
+    }
+    P.layers[P.n_layers++] = L;
+  }
+  P.layers[P.n_layers - 1].fin = 1;
+  // V_last: the 3 x 64 output layer in FP32, [c][j]
+  P.vlast_off = (uint32_t)off;
+  const size_t vbytes = kVlastFloats * 4;
+  if (blob) blob->resize(off + vbytes, 0);
+  if (fill) {
+    const float* w = vlast_src(d, cn);
+    const int n_in = d.cn_in[d.cn_nl - 1];
+    const float inv = eb == 2 ? 1.f : 1.f / dscale[P.n_layers - 1];
+    for (int c = 0; c < 3; ++c)
+      for (int j = 0; j < 64; ++j) {
+        const float v = j < n_in ? w[(size_t)c * n_in + j] * inv : 0.f;
+        std::memcpy(blob->data() + off + (c * 64 + j) * 4, &v, 4);
+      }
+  }
+  off += vbytes;
+  off = (off + 127) & ~size_t(127);
+  if (blob) blob->resize(off, 0);
+  P.blob_bytes = (uint32_t)off;
+  return P;
+}
+
+TcPlan plan_bf16(const NetDims& d, const float* op, const float* cn, std::vector<uint8_t>* blob) {
+  return make_plan(d, op, cn, 2, {}, {}, blob);
+}
 
 bool plan_supported(const NetDims& d, std::string* why) {
   auto no = [&](const char* m) { if (why) *why = m; return false; };
@@ -562,91 +787,83 @@ bool plan_supported(const NetDims& d, std::string* why) {
   return true;
 }
 
-Plan make_plan(const NetDims& d, const float* op, const float* cn) {
-  Plan P;
-  size_t off = 0;
-  const bool fill = op && cn;
-  auto add = [&](const float* W, int n, int k_total, int col0, int kc, bool relu) {
-    TcLayer L{};
-    const int np = pad16(n), kp = pad16(kc);
-    L.b_off = (uint32_t)off;
-    L.b_sbo = (uint32_t)kp * 16u;
-    L.k = kp;
-    L.n = np;
-    L.relu = relu;
-    if (fill) put_b(&P.blob, off, W, n, k_total, col0, kc, np, kp);
-    off += (size_t)np * kp * 2;
-    off = (off + 127) & ~size_t(127);
-    P.layers[P.n_layers++] = L;
-    return P.n_layers - 1;
-  };
-  const float* w = op;
-  for (int i = 0; i < d.op_nl; ++i) {
-    add(w, d.op_outs[i], d.op_in[i], 0, d.op_in[i], i + 1 < d.op_nl);
-    if (w) w += (size_t)d.op_in[i] * d.op_outs[i];
-  }
-  w = cn;
-  for (int i = 0; i + 1 < d.cn_nl; ++i) {
-    int li;
-    if (i == 0) {
-      li = add(w, d.cn_outs[0], d.cn_in[0], 0, d.op_out, true);
-      // aux block: columns [op_out, op_out + 16) of cmp_net's first layer
-      P.layers[li].aux = 1;
-      P.layers[li].aux_off = (uint32_t)off;
-      const int np = pad16(d.cn_outs[0]);
-      if (fill) put_b(&P.blob, off, w, d.cn_outs[0], d.cn_in[0], d.op_out, 16, np, 16);
-      off += (size_t)np * 16 * 2;
-      off = (off + 127) & ~size_t(127);
-    } else {
-      li = add(w, d.cn_outs[i], d.cn_in[i], 0, d.cn_in[i], true);
-    }
-    if (w) w += (size_t)d.cn_in[i] * d.cn_outs[i];
-  }
-  P.layers[P.n_layers - 1].fin = 1;
-  // V_last: the 3 x 64 output layer in FP32, [c][j]
-  P.vlast_off = (uint32_t)off;
-  const size_t vbytes = kVlastFloats * 4;
-  P.blob.resize((off + vbytes) / 2, 0);
-  if (fill) {
-    const int n_in = d.cn_in[d.cn_nl - 1];
-    for (int c = 0; c < 3; ++c)
-      for (int j = 0; j < 64; ++j) {
-        const float v = j < n_in ? w[(size_t)c * n_in + j] : 0.f;
-        std::memcpy(reinterpret_cast<char*>(P.blob.data()) + off + (c * 64 + j) * 4, &v, 4);
-      }
-  }
-  off += vbytes;
-  off = (off + 127) & ~size_t(127);
-  P.blob.resize(off / 2, 0);
-  return P;
-}
-
 }  // namespace
 
 bool relight_tc_supported(const NetDims& d, std::string* why) { return plan_supported(d, why); }
 
-size_t tc_weight_bytes(const NetDims& d) { return make_plan(d, nullptr, nullptr).blob.size() * 2; }
+bool relight_tc_fp8_supported(const NetDims& d, std::string* why) {
+  if (!plan_supported(d, why)) return false;
+  // every FP8 operand pads to K = 32 (zero columns); the widths above already do
+  return true;
+}
+
+int tc_layer_count(const NetDims& d) { return d.op_nl + d.cn_nl - 1; }
+
+size_t tc_weight_bytes(const NetDims& d) { return plan_bf16(d, nullptr, nullptr, nullptr).blob_bytes; }
 
 void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out) {
-  *out = make_plan(d, op, cn).blob;
+  std::vector<uint8_t> b;
+  plan_bf16(d, op, cn, &b);
+  out->assign(b.size() / 2, 0);
+  std::memcpy(out->data(), b.data(), b.size());
+}
+
+// Per-layer FP8 scales.  h[l] = kTarget / amax[l] maps layer l's input activations to
+// E4M3 with kTarget (half the format's range) at the calibrated maximum, leaving headroom
+// for values the calibration batch did not reach.  Layer l's weights carry
+// g[l] = h[l+1] / h[l], so its FP32 accumulator already equals the next layer's scaled
+// input and the epilogue converts it without a multiply; when that would push the weights
+// outside E4M3's range, g[l] is clamped and the epilogue multiplies by the remainder.
+// The fin layer's weights use the full range; V_last absorbs its accumulator scale.
+TcPlan pack_tc_weights_fp8(const NetDims& d, const float* op, const float* cn, const float* amax,
+                           std::vector<uint8_t>* out) {
+  constexpr float kTarget = 240.f, kWmax = 240.f, kWmin = 1.f / 16.f;
+  const std::vector<LayerSrc> src = layer_sources(d, op, cn);
+  const int n = (int)src.size();
+  std::vector<float> h(n), g(n), epi(n, 1.f), dscale(n);
+  for (int l = 0; l < n; ++l) h[l] = amax[l] > 0.f && std::isfinite(amax[l]) ? kTarget / amax[l] : 1.f;
+  for (int l = 0; l < n; ++l) {
+    const LayerSrc& ls = src[l];
+    float wmax = 0.f;
+    for (int r = 0; r < ls.n; ++r)
+      for (int c = 0; c < ls.kc; ++c) wmax = std::max(wmax, std::fabs(ls.w[(size_t)r * ls.k_total + ls.col0 + c]));
+    if (wmax == 0.f) wmax = 1.f;
+    if (l + 1 < n) {
+      g[l] = h[l + 1] / h[l];
+      const float lo = kWmin / wmax, hi = kWmax / wmax;
+      const float gc = std::min(std::max(g[l], lo), hi);
+      epi[l] = g[l] / gc;  // 1 unless clamped
+      g[l] = gc;
+    } else {
+      g[l] = kWmax / wmax;
+    }
+    dscale[l] = h[l] * g[l];  // accumulator = true pre-activation * dscale
+  }
+  out->clear();
+  TcPlan P = make_plan(d, op, cn, 1, g, dscale, out);
+  for (int l = 0; l < n; ++l) P.layers[l].scale = epi[l];
+  P.cp_scale = h[0];
+  return P;
 }
 
 size_t relight_tc_smem_bytes(const NetDims& d) {
   return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + sizeof(TcBarriers);
 }
 
-void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const uint16_t* tc_weights_dev,
-                       const TcJob* jobs, int n_jobs, TcJob* jobs_dev, int kahan, int clamp, uint32_t* err,
-                       cudaStream_t st) {
+void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
+                       const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, TcJob* jobs_dev, int kahan,
+                       int clamp, uint32_t* amax, uint32_t* err, cudaStream_t st) {
   std::string why;
   if (!plan_supported(d, &why)) fail(NWPRT_UNSUPPORTED, why);
   if (n_jobs <= 0) return;
-  Plan P = make_plan(d, nullptr, nullptr);
+  if (mode == kTcFp8 && !plan) fail(NWPRT_NOT_READY, "FP8 relight without a calibrated plan");
+  if (mode == kTcCalibrate && !amax) fail(NWPRT_INVALID_ARG, "calibration needs an amax buffer");
+  const TcPlan P = mode == kTcFp8 ? *plan : plan_bf16(d, nullptr, nullptr, nullptr);
   TcParams p{};
   p.hl = hl;
   p.hash = hash;
-  p.wblob = reinterpret_cast<const uint4*>(tc_weights_dev);
-  p.wblob_bytes = (uint32_t)(P.blob.size() * 2);
+  p.wblob = reinterpret_cast<const uint4*>(blob_dev);
+  p.wblob_bytes = P.blob_bytes;
   p.vlast_off = P.vlast_off;
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
   p.n_layers = P.n_layers;
@@ -654,6 +871,8 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.n_jobs = n_jobs;
   p.kahan = kahan;
   p.clamp = clamp;
+  p.cp_scale = P.cp_scale;
+  p.amax = amax;
   p.err = err;
   // tile prefix over the jobs, then one copy of the job table (stream ordered)
   std::vector<TcJob> J(jobs, jobs + n_jobs);
@@ -670,18 +889,20 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   NWPRT_CUDA(cudaGetDevice(&dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const size_t smem = relight_tc_smem_bytes(d);
+  const size_t smem = ((P.blob_bytes + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + sizeof(TcBarriers);
   if (smem > (size_t)max_smem) fail(NWPRT_UNSUPPORTED, "tensor-core relight: shared memory budget exceeded");
   const long long groups = (tiles + kNWG - 1) / kNWG;
   const int grid = (int)(groups < sms ? groups : sms);
-  if (d.enc_dims() <= 16) {
-    auto k = relight_tc_kernel<16>;
-    NWPRT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, st>>>(p);
-  } else {
-    auto k = relight_tc_kernel<32>;
-    NWPRT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, st>>>(p);
+  auto go = [&](auto kern) {
+    NWPRT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, kThreads, smem, st>>>(p);
+  };
+  const bool wide = d.enc_dims() > 16;
+  switch (mode) {
+    case kTcBf16: wide ? go(relight_tc_kernel<32, kTcBf16>) : go(relight_tc_kernel<16, kTcBf16>); break;
+    case kTcCalibrate: wide ? go(relight_tc_kernel<32, kTcCalibrate>) : go(relight_tc_kernel<16, kTcCalibrate>); break;
+    case kTcFp8: wide ? go(relight_tc_kernel<32, kTcFp8>) : go(relight_tc_kernel<16, kTcFp8>); break;
+    default: fail(NWPRT_INVALID_ARG, "unknown tensor-core mode");
   }
   NWPRT_CUDA(cudaGetLastError());
 }

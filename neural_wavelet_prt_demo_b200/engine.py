@@ -52,12 +52,12 @@ class RenderConfig:
     """renderConfig (RenderEngine.h:29-42) fields that matter to the relight, plus
     the arithmetic of the transport MLP."""
     waveletMode: bool = True
-    precision: str = "fp32"        # "fp32" (drop-in) | "bf16" (tcgen05)
+    precision: str = "fp32"        # "fp32" (drop-in) | "bf16" | "fp8" (tcgen05; fp8 after calibrateFP8)
     clamp_terms: bool = True       # utils_kernels.h:87-89 max(L*T, 0)
     kahan: bool = True
 
     def opts(self) -> _lib.RelightOpts:
-        prec = {"fp32": _lib.PREC_FP32, "bf16": _lib.PREC_BF16}.get(self.precision)
+        prec = {"fp32": _lib.PREC_FP32, "bf16": _lib.PREC_BF16, "fp8": _lib.PREC_FP8}.get(self.precision)
         if prec is None:
             raise ValueError(f"unknown precision {self.precision!r}")
         return _lib.RelightOpts(prec, int(self.clamp_terms), int(self.kahan))
@@ -300,6 +300,21 @@ class RenderEngine:
         opts = config.opts()
         self._check(lib().nwprt_relight_batch(self._ctx, arr, len(requests), C.byref(opts),
                                               _stream_ptr(stream)))
+
+    def calibrateFP8(self, envMapID: int, frameID: int, px_begin: int = 0, px_end: int = 0,
+                     stream=None) -> np.ndarray:
+        """Per-layer E4M3 scales from a BF16 pass over pixels [px_begin, px_end) of a prepared
+        frame; they stay fixed for every precision="fp8" relight until the next calibration
+        or weight load.  Blocking.  Returns the calibrated activation maxima."""
+        self._check(lib().nwprt_calibrate_fp8(self._ctx, int(envMapID), int(frameID), int(px_begin), int(px_end),
+                                              _stream_ptr(stream)))
+        return self.fp8Calibration()
+
+    def fp8Calibration(self) -> np.ndarray:
+        n = C.c_int(0)
+        buf = (C.c_float * 32)()
+        self._check(lib().nwprt_get_fp8_calibration(self._ctx, buf, 32, C.byref(n)))
+        return np.array(buf[:n.value], np.float32)
 
     def relightRanges(self, ranges, config: Optional[RenderConfig] = None, stream=None) -> None:
         """Pixel-range relights (envMapID, frameID, indirect, with_direct, px_begin, px_end) in
