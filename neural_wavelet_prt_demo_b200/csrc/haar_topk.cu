@@ -10,11 +10,14 @@
 //  * order = key descending, flat index face*S*S + row*S + col ascending.
 //
 // Design: a cluster of 6 CTAs (one per face) keeps every face in its own shared
-// memory.  The top-K threshold is found by a 4-pass 8-bit radix select whose
-// per-face histograms are summed through distributed shared memory; ties at the
-// threshold are taken in flat-index order by an ordered block compaction; the K
-// winners are gathered into CTA 0's shared memory and ranked there.  Nothing but
-// the inputs and outputs touches global memory.
+// memory: one bulk copy brings the face in, and every Haar level runs in place (operands
+// to registers, barrier, results back).  The top-K threshold is found by a 4-pass 8-bit
+// radix select: each CTA histograms its face, the cluster totals are summed through
+// distributed shared memory (the six remote loads issued together), and every CTA scans
+// the totals redundantly, so a pass costs one cluster barrier.  Ties at the threshold are
+// taken in flat-index order (one ordered block scan over the tie flags); the winners are
+// written into CTA 0's shared memory and ranked there.  Nothing but the inputs and
+// outputs touches global memory.
 #include <cooperative_groups.h>
 
 #include "nwprt_internal.cuh"
@@ -28,6 +31,8 @@ constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxS = 64;
 constexpr int kMaxK = 1024;
+constexpr int kMaxPerThread = kMaxS * kMaxS / kThreads;            // keys per thread in the compaction
+constexpr int kMaxLevelQuads = (kMaxS / 2) * (kMaxS / 2) / kThreads;  // 2x2 Haar blocks per thread
 
 struct Gathered {
   float r, g, b;
@@ -35,15 +40,16 @@ struct Gathered {
 };
 
 struct HaarSmem {
-  float* C;        // [S][S][3] coefficients
-  float* Tm;       // [(S/2)^2][3] level scratch
-  uint32_t* keys;  // [S*S]
-  uint32_t* hist;  // [2][256]
-  uint32_t* all_h; // [6][256] local copy of the cluster's histograms
-  uint64_t* gkey;  // [K] composite keys (CTA 0)
-  Gathered* gval;  // [K]
-  int* warp_tot;   // [kWarps]
-  int* scal;       // scalars
+  float* C;         // [S][S][3] the face, then its coefficients (in place)
+  uint32_t* keys;   // [S*S]
+  uint32_t* hist;   // [2][256] this face's histogram of the pass (double buffered)
+  uint32_t* all_h;  // [6][256] the cluster's histograms of the pass
+  uint32_t* tot;    // [256] their sum
+  uint64_t* gkey;   // [K] composite keys (CTA 0)
+  Gathered* gval;   // [K]
+  int* warp_tot;    // [kWarps]
+  int* scal;        // scalars
+  uint64_t* bar;    // bulk-copy completion
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -52,24 +58,26 @@ __host__ __device__ inline size_t smem_layout(int S, int K, char* base, HaarSmem
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t at = o; o = align16(o + bytes); return at; };
   size_t oC = take(sizeof(float) * S * S * 3);
-  size_t oT = take(sizeof(float) * (S / 2 > 0 ? (S / 2) * (S / 2) : 1) * 3);
   size_t oK = take(sizeof(uint32_t) * S * S);
   size_t oH = take(sizeof(uint32_t) * 512);
   size_t oA = take(sizeof(uint32_t) * 6 * 256);
+  size_t oT = take(sizeof(uint32_t) * 256);
   size_t oG = take(sizeof(uint64_t) * K);
   size_t oV = take(sizeof(Gathered) * K);
   size_t oW = take(sizeof(int) * kWarps);
   size_t oS = take(sizeof(int) * 32);
+  size_t oB = take(sizeof(uint64_t));
   if (L) {
     L->C = (float*)(base + oC);
-    L->Tm = (float*)(base + oT);
     L->keys = (uint32_t*)(base + oK);
     L->hist = (uint32_t*)(base + oH);
     L->all_h = (uint32_t*)(base + oA);
+    L->tot = (uint32_t*)(base + oT);
     L->gkey = (uint64_t*)(base + oG);
     L->gval = (Gathered*)(base + oV);
     L->warp_tot = (int*)(base + oW);
     L->scal = (int*)(base + oS);
+    L->bar = (uint64_t*)(base + oB);
   }
   return o;
 }
@@ -93,13 +101,16 @@ __device__ __forceinline__ uint32_t wavelet_key_bits(float r, float g, float b) 
   return __float_as_uint(t);
 }
 
-// Exclusive rank of `pred` among the block's threads in thread order, plus the
-// block total.  Two __syncthreads.
-__device__ __forceinline__ int block_rank(bool pred, int* warp_tot, int* total) {
+// Exclusive prefix of `v` over the block's threads in thread order, plus the block total.
+__device__ __forceinline__ int block_exclusive_sum(int v, int* warp_tot, int* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned m = __ballot_sync(0xffffffffu, pred);
-  const int in_warp = __popc(m & ((1u << lane) - 1u));
-  if (lane == 0) warp_tot[warp] = __popc(m);
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
   __syncthreads();
   int before = 0, all = 0;
 #pragma unroll
@@ -110,12 +121,12 @@ __device__ __forceinline__ int block_rank(bool pred, int* warp_tot, int* total) 
   }
   __syncthreads();
   *total = all;
-  return before + in_warp;
+  return before + incl - v;
 }
 
 __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
     haar_topk_kernel(const float* __restrict__ faces, int S, int K, int32_t* __restrict__ idx_out,
-                     float* __restrict__ st_out) {
+                     float* __restrict__ st_out, uint32_t* err) {
   extern __shared__ __align__(16) char smem_raw[];
   HaarSmem sm;
   smem_layout(S, K, smem_raw, &sm);
@@ -123,51 +134,72 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
   const int face = (int)cluster.block_rank();
   const int env = blockIdx.x / 6;
   const int tid = threadIdx.x, nt = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31;
   const int SS = S * S;
   const float* src = faces + ((size_t)env * 6 + face) * (size_t)SS * 3;
 
-  // ---- level n = S, straight from global memory into C
-  if (S >= 2) {
-    const int h = S >> 1;
-    for (int b = tid; b < h * h; b += nt) {
-      const int i = b / h, j = b - i * h;
-      const float* r0 = src + ((size_t)(2 * i) * S + 2 * j) * 3;
-      const float* r1 = r0 + (size_t)S * 3;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float ll, hl, lh, hh;
-        haar4(__ldg(r0 + c), __ldg(r0 + 3 + c), __ldg(r1 + c), __ldg(r1 + 3 + c), ll, hl, lh, hh);
-        sm.C[(i * S + j) * 3 + c] = ll;
-        sm.C[(i * S + j + h) * 3 + c] = hl;
-        sm.C[((i + h) * S + j) * 3 + c] = lh;
-        sm.C[((i + h) * S + j + h) * 3 + c] = hh;
-      }
+  // ---- the face into shared memory: one bulk copy when the source allows it
+  const uint32_t face_bytes = (uint32_t)SS * 12u;
+  const bool bulk = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (face_bytes % 16 == 0);
+  if (bulk) {
+    if (tid == 0) {
+      mbar_init(sm.bar, 1);
+      fence_barrier_init();
     }
+    __syncthreads();
+    if (tid == 0) {
+      mbar_arrive_expect_tx(sm.bar, face_bytes);
+      bulk_g2s(sm.C, src, face_bytes, sm.bar);
+    }
+    // on a timeout the face reads as whatever is in shared memory; the error is reported
+    // and every CTA still reaches the cluster barriers below
+    mbar_wait(sm.bar, 0, err);
   } else {
-    if (tid < 3) sm.C[tid] = src[tid];
+    for (int e = tid; e < SS * 3; e += nt) sm.C[e] = __ldg(src + e);
+    __syncthreads();
   }
-  __syncthreads();
-  // ---- remaining levels inside shared memory
-  for (int n = S >> 1; n >= 2; n >>= 1) {
+  // ---- Haar levels n = S, S/2, ..., 2 in place on the top-left n x n block: each thread
+  // reads its 2x2 blocks (3 channels, two 8-byte-aligned runs of 6 floats), then after a
+  // barrier writes their LL, HL, LH, HH
+  for (int n = S, lg = 0; n >= 2; n >>= 1) {
     const int h = n >> 1;
-    for (int b = tid; b < h * h; b += nt) {
-      const int i = b / h, j = b - i * h;
+    while ((1 << lg) < h) ++lg;
+    while ((1 << lg) > h) --lg;
+    float in[kMaxLevelQuads][12];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float ll, hl, lh, hh;
-        haar4(sm.C[((2 * i) * S + 2 * j) * 3 + c], sm.C[((2 * i) * S + 2 * j + 1) * 3 + c],
-              sm.C[((2 * i + 1) * S + 2 * j) * 3 + c], sm.C[((2 * i + 1) * S + 2 * j + 1) * 3 + c],
-              ll, hl, lh, hh);
-        sm.Tm[(i * n + j) * 3 + c] = ll;
-        sm.Tm[(i * n + j + h) * 3 + c] = hl;
-        sm.Tm[((i + h) * n + j) * 3 + c] = lh;
-        sm.Tm[((i + h) * n + j + h) * 3 + c] = hh;
+    for (int u = 0; u < kMaxLevelQuads; ++u) {
+      const int b = tid + u * nt;
+      if (b < h * h) {
+        const int i = b >> lg, j = b & (h - 1);
+        const float2* r0 = reinterpret_cast<const float2*>(sm.C + ((2 * i) * S + 2 * j) * 3);
+        const float2* r1 = reinterpret_cast<const float2*>(sm.C + ((2 * i + 1) * S + 2 * j) * 3);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float2 x = r0[q], y = r1[q];
+          in[u][2 * q] = x.x;
+          in[u][2 * q + 1] = x.y;
+          in[u][6 + 2 * q] = y.x;
+          in[u][6 + 2 * q + 1] = y.y;
+        }
       }
     }
     __syncthreads();
-    for (int e = tid; e < n * n * 3; e += nt) {
-      const int r = e / (n * 3), rem = e - r * (n * 3);
-      sm.C[r * S * 3 + rem] = sm.Tm[e];
+#pragma unroll
+    for (int u = 0; u < kMaxLevelQuads; ++u) {
+      const int b = tid + u * nt;
+      if (b < h * h) {
+        const int i = b >> lg, j = b & (h - 1);
+        // in[]: row 2i = (px 2j: r g b, px 2j+1: r g b), then row 2i+1 likewise
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float ll, hl, lh, hh;
+          haar4(in[u][c], in[u][3 + c], in[u][6 + c], in[u][9 + c], ll, hl, lh, hh);
+          sm.C[(i * S + j) * 3 + c] = ll;
+          sm.C[(i * S + j + h) * 3 + c] = hl;
+          sm.C[((i + h) * S + j) * 3 + c] = lh;
+          sm.C[((i + h) * S + j + h) * 3 + c] = hh;
+        }
+      }
     }
     __syncthreads();
   }
@@ -182,6 +214,7 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
   for (int pass = 0; pass < 4; ++pass) {
     const int shift = 24 - 8 * pass;
     uint32_t* h = sm.hist + (pass & 1) * 256;
+    // buffer (pass & 1) was last read remotely in pass - 2, before the previous cluster barrier
     for (int d = tid; d < 256; d += nt) h[d] = 0;
     __syncthreads();
     for (int p = tid; p < SS; p += nt) {
@@ -190,23 +223,27 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
     }
     cluster.sync();
     if (tid < 256) {
+      uint32_t v[6];
 #pragma unroll
-      for (int g = 0; g < 6; ++g) sm.all_h[g * 256 + tid] = cluster.map_shared_rank(h, g)[tid];
+      for (int g = 0; g < 6; ++g) v[g] = cluster.map_shared_rank(h, g)[tid];
+      uint32_t t = 0;
+#pragma unroll
+      for (int g = 0; g < 6; ++g) {
+        sm.all_h[g * 256 + tid] = v[g];
+        t += v[g];
+      }
+      sm.tot[tid] = t;
     }
     __syncthreads();
-    if (tid < 32) {
+    if (warp == 0) {
       // lane l covers digits 255-8l .. 248-8l (highest digits first)
-      const int lane = tid;
       const int d_hi = 255 - 8 * lane;
       uint32_t tot8[8];
       uint32_t local = 0;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        uint32_t t = 0;
-#pragma unroll
-        for (int g = 0; g < 6; ++g) t += sm.all_h[g * 256 + d_hi - q];
-        tot8[q] = t;
-        local += t;
+        tot8[q] = sm.tot[d_hi - q];
+        local += tot8[q];
       }
       uint32_t incl = local;
 #pragma unroll
@@ -229,33 +266,37 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
       }
       dsel = __shfl_sync(0xffffffffu, dsel, cl);
       above = __shfl_sync(0xffffffffu, above, cl);
-      // per-face counts of keys whose digit is above dsel
-#pragma unroll
-      for (int g = 0; g < 6; ++g) {
-        uint32_t s = 0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int d = d_hi - q;
-          s += d > dsel ? sm.all_h[g * 256 + d] : 0u;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) {
-          gt[g] += (int)s;
-          if (pass == 3) eq[g] = (int)sm.all_h[g * 256 + dsel];
-        }
-      }
       if (lane == 0) {
         sm.scal[0] = (int)(prefix | ((uint32_t)dsel << shift));
         sm.scal[1] = (int)(mask | (255u << shift));
         sm.scal[2] = remaining - (int)above;
+        sm.scal[3] = dsel;
       }
     }
     __syncthreads();
     prefix = (uint32_t)sm.scal[0];
     mask = (uint32_t)sm.scal[1];
     remaining = sm.scal[2];
+    // per-face counts of keys whose digit is above the selected one (warp g: face g)
+    if (warp < 6) {
+      const int dsel = sm.scal[3];
+      const int d_hi = 255 - 8 * lane;
+      uint32_t s = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int d = d_hi - q;
+        s += d > dsel ? sm.all_h[warp * 256 + d] : 0u;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) {
+        gt[warp] += (int)s;
+        if (pass == 3) eq[warp] = (int)sm.all_h[warp * 256 + dsel];
+      }
+    }
+    // the next pass starts with a barrier; the loop's last one follows below
   }
+  __syncthreads();
   // ---- this face's share of the winners
   const uint32_t thr = prefix;
   int eq_before = 0, n_before = 0;
@@ -269,26 +310,35 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
   take = take < 0 ? 0 : (take > eq[face] ? eq[face] : take);
   uint64_t* dkey = cluster.map_shared_rank(sm.gkey, 0);
   Gathered* dval = cluster.map_shared_rank(sm.gval, 0);
-  int base_tie = 0, base_sel = 0;
-  for (int p0 = 0; p0 < SS; p0 += nt) {
-    const int p = p0 + tid;
-    const uint32_t k = p < SS ? sm.keys[p] : 0u;
-    const bool is_tie = p < SS && k == thr;
-    const bool is_gt = p < SS && k > thr;
-    int n_tie;
-    const int tie_rank = base_tie + block_rank(is_tie, sm.warp_tot, &n_tie);
-    const bool sel = is_gt || (is_tie && tie_rank < take);
-    int n_sel;
-    const int sel_rank = base_sel + block_rank(sel, sm.warp_tot, &n_sel);
+  // thread t owns keys [t*per, t*per + per): ties get their flat-index rank from one
+  // ordered scan; the winners' slots in CTA 0 only need to be distinct (the final rank
+  // orders them), so they come from a shared counter
+  const int per = (SS + nt - 1) / nt;
+  const int p0 = tid * per;
+  int n_tie_mine = 0;
+#pragma unroll
+  for (int u = 0; u < kMaxPerThread; ++u) {
+    const int p = p0 + u;
+    if (u < per && p < SS && sm.keys[p] == thr) ++n_tie_mine;
+  }
+  int *counter = sm.scal + 24;
+  if (tid == 0) *counter = 0;
+  int n_tie_all;
+  int tie_rank = block_exclusive_sum(n_tie_mine, sm.warp_tot, &n_tie_all);
+#pragma unroll
+  for (int u = 0; u < kMaxPerThread; ++u) {
+    const int p = p0 + u;
+    if (u >= per || p >= SS) continue;
+    const uint32_t k = sm.keys[p];
+    bool sel = k > thr;
+    if (k == thr) sel = tie_rank++ < take;
     if (sel) {
-      const int slot = n_before + sel_rank;
+      const int slot = n_before + atomicAdd(counter, 1);
       const int32_t flat = face * SS + p;
       // composite key: larger key first, then smaller index first
       dkey[slot] = ((uint64_t)k << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)flat);
       dval[slot] = Gathered{sm.C[p * 3], sm.C[p * 3 + 1], sm.C[p * 3 + 2], flat};
     }
-    base_tie += n_tie;
-    base_sel += n_sel;
   }
   cluster.sync();
   // ---- rank the K winners (CTA 0)
@@ -313,7 +363,6 @@ size_t haar_topk_smem_bytes(int S, int K) { return smem_layout(S, K, nullptr, nu
 
 void launch_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx, float* strength,
                       uint32_t* err, cudaStream_t st) {
-  (void)err;
   if (n_env < 1 || n_env > (1 << 28)) fail(NWPRT_INVALID_ARG, "haar_topk: n_env out of range");
   if (S < 1 || S > kMaxS || (S & (S - 1)))
     fail(S > kMaxS ? NWPRT_UNSUPPORTED : NWPRT_INVALID_ARG,
@@ -323,7 +372,7 @@ void launch_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx,
   if (!faces || !idx || !strength) fail(NWPRT_INVALID_ARG, "haar_topk: null pointer");
   const size_t smem = haar_topk_smem_bytes(S, K);
   NWPRT_CUDA(cudaFuncSetAttribute(haar_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  haar_topk_kernel<<<6 * n_env, kThreads, smem, st>>>(faces, S, K, idx, strength);
+  haar_topk_kernel<<<6 * n_env, kThreads, smem, st>>>(faces, S, K, idx, strength, err);
   NWPRT_CUDA(cudaGetLastError());
 }
 
