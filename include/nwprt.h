@@ -218,6 +218,12 @@ NWPRT_API nwprt_status nwprt_haar_topk(const float* faces, int n_env, int S, int
  * Feeds rotated env maps to nwprt_env_from_faces (the reference precomputes such
  * rotations offline, README "EnvmapRotation" sets). */
 NWPRT_API nwprt_status nwprt_env_rotate(const float* src, int S, const float* R, float* dst, void* stream);
+/* Final colour of a relit frame -- RenderEngine::computeFinalPixelColors
+ * (Renderer/toneMap.cu:47-98) on fbPredictedIndirectWithDirect or fbPredictedIndirect:
+ * per channel 1.055 (x + 1e-6)^(1/2.4) - 0.055, clamped to [0, 1], times 255.9, truncated;
+ * packed r | g << 8 | b << 16 | 255 << 24.  src: n_px float4 (16-byte aligned), dst: n_px
+ * uint32, both device memory. */
+NWPRT_API nwprt_status nwprt_tonemap_srgb(const float* src, int64_t n_px, uint32_t* dst, void* stream);
 /* SH projection (order 8, 81 coefficients) of a cubemap [6][S][S][3] -> L[81][3]
  * (the env SH the reference loads from sh/<name>.npy, EnvironmentMap.cpp:70-77).
  * `workspace` must hold nwprt_sh_project_workspace_size(S) bytes of device memory. */

@@ -678,6 +678,10 @@ nwprt_status nwprt_get_fp8_calibration(const nwprt_ctx* ctx, float* amax, int ca
   });
 }
 
+nwprt_status nwprt_tonemap_srgb(const float* src, int64_t n_px, uint32_t* dst, void* stream) {
+  return guarded(nullptr, [&] { launch_tonemap_srgb(src, n_px, dst, (cudaStream_t)stream); });
+}
+
 nwprt_status nwprt_sync(nwprt_ctx* ctx) {
   return guarded(ctx, [&] {
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");

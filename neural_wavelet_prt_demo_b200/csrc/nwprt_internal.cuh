@@ -145,6 +145,9 @@ void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWei
 void pack_fp32_weights(const NetDims& d, const float* op, const float* cn,
                        std::vector<float>* op_t, std::vector<float>* cn_t);
 
+// tonemap.cu
+void launch_tonemap_srgb(const float* src, int64_t n, uint32_t* dst, cudaStream_t st);
+
 // relight_tc.cu (tcgen05 path: BF16 operands, or FP8 e4m3 with per-layer scales)
 constexpr int kMaxTcLayers = 12;
 // One tensor-core layer of the per-wavelet MLP chain (B operand offsets inside the weight blob).
@@ -238,11 +241,9 @@ __host__ __device__ inline float float_from_bits(uint32_t u) {
   return f;
 }
 
-__host__ __device__ inline float logf_series(float xf) {
-  if (xf != xf) return xf;
-  if (xf < 0.0f) return float_from_bits(0x7fc00000u);
-  if (xf == 0.0f) return float_from_bits(0xff800000u);
-  if (xf > 3.4028234663852886e38f) return xf;
+// ln(x) in double for a positive finite float x, by the series above; the exponent part
+// is returned separately so that logf_series rounds exactly as before.
+__host__ __device__ inline double log_series_mantissa(float xf, int* exponent) {
   const double x = (double)xf;
   unsigned long long b;
   memcpy(&b, &x, 8);
@@ -265,8 +266,66 @@ __host__ __device__ inline float logf_series(float xf) {
   p = fma(p, z, 1.0 / 5.0);
   p = fma(p, z, 1.0 / 3.0);
   p = fma(p, z, 1.0);
-  const double lm = (2.0 * s) * p;
+  *exponent = e;
+  return (2.0 * s) * p;
+}
+
+__host__ __device__ inline float logf_series(float xf) {
+  if (xf != xf) return xf;
+  if (xf < 0.0f) return float_from_bits(0x7fc00000u);
+  if (xf == 0.0f) return float_from_bits(0xff800000u);
+  if (xf > 3.4028234663852886e38f) return xf;
+  int e;
+  const double lm = log_series_mantissa(xf, &e);
   return (float)fma((double)e, 0.6931471805599453, lm);
+}
+
+// x^y of a float by exp(y ln x) in IEEE double, rounded once to float: ln from the series
+// above, exp by reduction t = k ln2 + r (|r| <= ln2/2) and the Taylor series of e^r to r^18
+// (truncation error < 1e-22).  Every step is an explicit fma or a single IEEE operation, so
+// host, device and the CPU oracle return the same bits.  Negative x gives NaN, 0 gives 0
+// (y > 0), +inf gives +inf -- as powf for y in (0, 1).
+__host__ __device__ inline float powf_series(float xf, float yf) {
+  if (xf != xf || xf < 0.0f) return float_from_bits(0x7fc00000u);
+  if (xf == 0.0f) return 0.0f;
+  if (xf > 3.4028234663852886e38f) return xf;
+  int e;
+  const double lm = log_series_mantissa(xf, &e);
+  const double t = fma((double)e, 0.6931471805599453, lm) * (double)yf;
+  const double kd = floor(fma(t, 1.4426950408889634, 0.5));
+  const double r = fma(-kd, 0.6931471805599453, t);
+  double p = 1.0 / 6402373705728000.0;  // 1/18!
+  p = fma(p, r, 1.0 / 355687428096000.0);
+  p = fma(p, r, 1.0 / 20922789888000.0);
+  p = fma(p, r, 1.0 / 1307674368000.0);
+  p = fma(p, r, 1.0 / 87178291200.0);
+  p = fma(p, r, 1.0 / 6227020800.0);
+  p = fma(p, r, 1.0 / 479001600.0);
+  p = fma(p, r, 1.0 / 39916800.0);
+  p = fma(p, r, 1.0 / 3628800.0);
+  p = fma(p, r, 1.0 / 362880.0);
+  p = fma(p, r, 1.0 / 40320.0);
+  p = fma(p, r, 1.0 / 5040.0);
+  p = fma(p, r, 1.0 / 720.0);
+  p = fma(p, r, 1.0 / 120.0);
+  p = fma(p, r, 1.0 / 24.0);
+  p = fma(p, r, 1.0 / 6.0);
+  p = fma(p, r, 0.5);
+  p = fma(p, r, 1.0);
+  p = fma(p, r, 1.0);
+  return (float)ldexp(p, (int)kd);
+}
+
+// sRGB-style encode of one linear channel to a byte, as the reference's final-colour pass
+// does it (Renderer/toneMap.cu:47-71): 1.055 (x + 1e-6)^(1/2.4) - 0.055, clamped to
+// [0, 1] (NaN -> 0), times 255.9, truncated.
+__host__ __device__ inline uint32_t srgb_byte(float x) {
+  const float coeff = 1.055f;
+  const float p = powf_series(x + 1e-6f, 1.0f / 2.4f);
+  float f = fmaf(coeff, p, -(coeff - 1.0f));
+  f = f > 0.0f ? f : 0.0f;  // NaN -> 0, like fmaxf(0, NaN)
+  f = f < 1.0f ? f : 1.0f;
+  return (uint32_t)(f * 255.9f);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {

@@ -78,6 +78,7 @@ class FullFrame:
     fbEnvironmentMapFlag: torch.Tensor
     fbPredictedIndirect: torch.Tensor
     fbPredictedIndirectWithDirect: torch.Tensor
+    fbFinalColor: Optional[torch.Tensor] = None   # int32 [n] packed RGBA8, by computeFinalPixelColors
 
     @staticmethod
     def from_gbuffer(gb, device="cuda:0") -> "FullFrame":
@@ -346,6 +347,19 @@ class RenderEngine:
         """tcnn.cu:154-158; also surfaces device-side error reports."""
         self._check(lib().nwprt_sync(self._ctx))
 
+    def computeFinalPixelColors(self, frameID: int, renderingMode: str = "full", stream=None) -> torch.Tensor:
+        """RenderEngine::computeFinalPixelColors (toneMap.cu:73-98) for the wavelet path: the
+        relit frame (indirect + direct for "full", indirect alone for "indirect") -> packed
+        RGBA8 in frame.fbFinalColor (int32 tensor holding the uint32 pixels).  Asynchronous."""
+        fr = self.fullframeCUDABuffer[frameID]
+        src = {"full": fr.fbPredictedIndirectWithDirect, "indirect": fr.fbPredictedIndirect}.get(renderingMode)
+        if src is None:
+            raise ValueError(f"unknown renderingMode {renderingMode!r}")
+        n = fr.width * fr.height
+        if fr.fbFinalColor is None or fr.fbFinalColor.numel() != n:
+            fr.fbFinalColor = torch.empty(n, dtype=torch.int32, device=src.device)
+        return tonemap_srgb(src, out=fr.fbFinalColor, stream=stream)
+
 
 # -------------------------------------------------------------------- context-free kernels
 
@@ -360,6 +374,20 @@ def haar_topk(faces: torch.Tensor, K: int, stream=None):
     st = torch.empty((E, K, 3), dtype=torch.float32, device=faces.device)
     check(lib().nwprt_haar_topk(_ptr(f), E, S, int(K), _ptr(idx), _ptr(st), _stream_ptr(stream)))
     return (idx, st) if batched else (idx[0], st[0])
+
+
+def tonemap_srgb(src: torch.Tensor, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+    """float32 cuda [n, 4] linear radiance -> int32 [n] packed RGBA8 (the reference's
+    final-colour pass, toneMap.cu:47-71)."""
+    if src.dtype != torch.float32 or not src.is_cuda or not src.is_contiguous() or src.shape[-1] != 4:
+        raise ValueError("src must be a contiguous float32 CUDA tensor [n, 4]")
+    n = src.numel() // 4
+    if out is None:
+        out = torch.empty(n, dtype=torch.int32, device=src.device)
+    if out.dtype != torch.int32 or out.numel() != n or not out.is_contiguous():
+        raise ValueError("out must be a contiguous int32 tensor of n pixels")
+    check(lib().nwprt_tonemap_srgb(_ptr(src), n, _ptr(out), _stream_ptr(stream)))
+    return out
 
 
 def env_rotate(faces: torch.Tensor, R, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:

@@ -303,6 +303,110 @@ float orc_logf_series(float xf) {
   return (float)fma((double)e, 0.6931471805599453, lm);
 }
 
+/* x^y = exp(y ln x) in IEEE double, rounded once to float: the logarithm by the atanh
+ * series of orc_logf_series (Abramowitz & Stegun 4.1.27), the exponential by reduction
+ * t = k ln2 + r, |r| <= ln2/2, and the Taylor series of e^r up to r^18.  The reference's
+ * final-colour pass calls powf (Renderer/toneMap.cu:33-39,61); this is the restatement
+ * the library evaluates on host and device. */
+float orc_powf_series(float xf, float yf) {
+  if (xf != xf || xf < 0.0f) return NAN;
+  if (xf == 0.0f) return 0.0f;
+  if (isinf(xf)) return xf;
+  double x = (double)xf;
+  uint64_t b;
+  memcpy(&b, &x, 8);
+  int e = (int)((b >> 52) & 0x7ff) - 1023;
+  b = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+  double m;
+  memcpy(&m, &b, 8);
+  if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 23.0;
+  p = fma(p, z, 1.0 / 21.0);
+  p = fma(p, z, 1.0 / 19.0);
+  p = fma(p, z, 1.0 / 17.0);
+  p = fma(p, z, 1.0 / 15.0);
+  p = fma(p, z, 1.0 / 13.0);
+  p = fma(p, z, 1.0 / 11.0);
+  p = fma(p, z, 1.0 / 9.0);
+  p = fma(p, z, 1.0 / 7.0);
+  p = fma(p, z, 1.0 / 5.0);
+  p = fma(p, z, 1.0 / 3.0);
+  p = fma(p, z, 1.0);
+  const double lm = (2.0 * s) * p;
+  const double t = fma((double)e, 0.6931471805599453, lm) * (double)yf;
+  const double kd = floor(fma(t, 1.4426950408889634, 0.5));
+  const double r = fma(-kd, 0.6931471805599453, t);
+  /* 1/n! for n = 18 .. 0 */
+  static const double inv_fact[19] = {
+      1.0 / 6402373705728000.0, 1.0 / 355687428096000.0, 1.0 / 20922789888000.0, 1.0 / 1307674368000.0,
+      1.0 / 87178291200.0, 1.0 / 6227020800.0, 1.0 / 479001600.0, 1.0 / 39916800.0, 1.0 / 3628800.0,
+      1.0 / 362880.0, 1.0 / 40320.0, 1.0 / 5040.0, 1.0 / 720.0, 1.0 / 120.0, 1.0 / 24.0, 1.0 / 6.0,
+      0.5, 1.0, 1.0};
+  double q = inv_fact[0];
+  for (int i = 1; i < 19; ++i) q = fma(q, r, inv_fact[i]);
+  return (float)ldexp(q, (int)kd);
+}
+
+/* One linear channel -> byte, Renderer/toneMap.cu:57-69: f = 1.055 (x + 1e-6)^(1/2.4) - 0.055
+ * (the multiply-subtract contracted to one fma, as nvcc compiles it), clamped to [0, 1] with
+ * NaN -> 0, times 255.9, truncated. */
+static uint32_t orc_srgb_byte(float x) {
+  const float coeff = 1.055f;
+  const float p = orc_powf_series(x + 1e-6f, 1.0f / 2.4f);
+  float f = fmaf(coeff, p, -(coeff - 1.0f));
+  f = f > 0.0f ? f : 0.0f;
+  f = f < 1.0f ? f : 1.0f;
+  return (uint32_t)(f * 255.9f);
+}
+
+/* computeFinalPixelColorsKernel (Renderer/toneMap.cu:47-71): float4 -> r | g<<8 | b<<16 | 255<<24. */
+void orc_tonemap_srgb(const float* src, int64_t n, uint32_t* dst) {
+  for (int64_t i = 0; i < n; ++i)
+    dst[i] = orc_srgb_byte(src[i * 4]) | (orc_srgb_byte(src[i * 4 + 1]) << 8) |
+             (orc_srgb_byte(src[i * 4 + 2]) << 16) | (255u << 24);
+}
+
+/* The 255 step thresholds of orc_srgb_byte: t[j] = the smallest float x >= 0 whose byte is
+ * >= j, by bisection over the ordered bit patterns of non-negative floats. */
+void orc_srgb_thresholds(float* t) {
+  t[0] = 0.0f;
+  for (int j = 1; j < 256; ++j) {
+    uint32_t lo = 0, hi = 0x7f800000u;
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      float x;
+      memcpy(&x, &mid, 4);
+      if (orc_srgb_byte(x) >= (uint32_t)j) hi = mid;
+      else lo = mid + 1;
+    }
+    memcpy(&t[j], &lo, 4);
+  }
+}
+
+/* Floats within `radius` ulps of every threshold (and all negative/NaN/inf specials) whose
+ * byte from the threshold count differs from the direct evaluation: 0 means the step table
+ * and the formula agree wherever the byte can change. */
+int64_t orc_srgb_threshold_mismatches(const float* t, int radius) {
+  int64_t bad = 0;
+  for (int j = 1; j < 256; ++j) {
+    uint32_t c;
+    memcpy(&c, &t[j], 4);
+    for (int64_t d = -radius; d <= radius; ++d) {
+      const int64_t b = (int64_t)c + d;
+      if (b < 0 || b > 0x7f800000LL) continue;
+      const uint32_t ub = (uint32_t)b;
+      float x;
+      memcpy(&x, &ub, 4);
+      uint32_t k = 0;
+      for (int i = 1; i < 256; ++i) k += t[i] <= x;
+      bad += k != orc_srgb_byte(x);
+    }
+  }
+  return bad;
+}
+
 /* The reference's per-pixel 16-float input row (waveletDataCopy,
  * utils_kernels.h:7-49; layout prt_globals.h:4-13):
  * pos(3) normal(3) reflect(3) log(25r+1)/log(26) 2kd-1(3) 2ks-1(3). */

@@ -79,6 +79,10 @@ void orc_sh_dot_f64(const float* T, int64_t N, int nc, const double* L, int abs_
 
 /* ---- relight pieces ---- */
 float orc_logf_series(float x);
+float orc_powf_series(float x, float y);
+void orc_tonemap_srgb(const float* src, int64_t n, uint32_t* dst);
+void orc_srgb_thresholds(float* t256);
+int64_t orc_srgb_threshold_mismatches(const float* t256, int radius);
 void orc_remap_f32(const orc_gbuf* g, int64_t px, float row[16]);
 void orc_hash_encode_f32(const orc_net* net, const float* hash, const float pos[3], float* out);
 void orc_hash_encode_f64(const orc_net* net, const float* hash, const float pos[3], double* out);

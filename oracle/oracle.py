@@ -157,6 +157,35 @@ def env_rotate(faces: np.ndarray, R: np.ndarray) -> np.ndarray:
     return out
 
 
+def powf_series(x, y) -> np.ndarray:
+    """Elementwise float x^y by the oracle's series (the arithmetic of the final-colour pass)."""
+    xs = np.ascontiguousarray(x, np.float32).ravel()
+    f = lib().orc_powf_series
+    f.restype = C.c_float
+    f.argtypes = [C.c_float, C.c_float]
+    return np.array([f(float(v), float(y)) for v in xs], np.float32).reshape(np.shape(x))
+
+
+def tonemap_srgb(src: np.ndarray) -> np.ndarray:
+    """float4 [n, 4] linear radiance -> uint32 [n] RGBA8 (Renderer/toneMap.cu:47-71)."""
+    s = np.ascontiguousarray(src, np.float32).reshape(-1, 4)
+    out = np.empty(s.shape[0], np.uint32)
+    lib().orc_tonemap_srgb(_p(s), C.c_int64(s.shape[0]), _p(out))
+    return out
+
+
+def srgb_thresholds() -> np.ndarray:
+    t = np.empty(256, np.float32)
+    lib().orc_srgb_thresholds(_p(t))
+    return t
+
+
+def srgb_threshold_mismatches(t: np.ndarray, radius: int) -> int:
+    f = lib().orc_srgb_threshold_mismatches
+    f.restype = C.c_int64
+    return int(f(_p(np.ascontiguousarray(t, np.float32)), C.c_int(radius)))
+
+
 def sh_eval_f64(d, lmax=8) -> np.ndarray:
     out = np.zeros((lmax + 1) ** 2, np.float64)
     lib().orc_sh_eval_f64(C.c_double(d[0]), C.c_double(d[1]), C.c_double(d[2]), C.c_int(lmax),

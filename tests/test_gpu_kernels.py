@@ -94,3 +94,45 @@ def test_sh_dot_1080p_sampled(cuda):
     rows = np.random.default_rng(0).choice(N, 4096, replace=False)
     ref = O.sh_dot_f32(T[rows].cpu().numpy(), L.cpu().numpy())
     assert np.array_equal(out[rows].cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_tonemap_bit_exact(cuda):
+    import torch
+    eng = _engine()
+    g = np.random.default_rng(11)
+    n = 300_001
+    x = np.concatenate([g.uniform(0, 1.5, n * 2), 10.0 ** g.uniform(-7, 2, n * 2)]).astype(np.float32)
+    src = x[: n * 4].reshape(n, 4).copy()
+    src[:16, :3] = np.array([0, 0.5, 1, -1, np.nan, np.inf, -np.inf, 1e-8, 3e38, 0.18, 2, 1e-3, 0.04,
+                             0.0031308, 0.99, 1.01], np.float32).reshape(16, 1)
+    # every step of the byte function, +-8 ulps
+    t = O.srgb_thresholds()[1:].view(np.int32)
+    near = (t[:, None] + np.arange(-8, 9, dtype=np.int32)[None, :]).ravel().view(np.float32)
+    src[16:16 + near.size // 3 * 1, :3] = np.resize(near, (near.size // 3 * 1, 3))
+    got = eng.tonemap_srgb(torch.from_numpy(src).to(cuda)).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, O.tonemap_srgb(src))
+    with pytest.raises(ValueError):
+        eng.tonemap_srgb(torch.zeros((4, 3), device=cuda))
+    assert eng.tonemap_srgb(torch.zeros((0, 4), device=cuda)).numel() == 0
+
+
+def test_final_pixel_colors_of_a_relit_frame(cuda):
+    from neural_wavelet_prt_demo_b200 import netconfig
+    from tests.helpers import make_case
+    eng = _engine()
+    case = make_case(netconfig.CONFIG_SMALL, 40, 24, 32, seed=4, hash_scale=0.5)
+    e = eng.RenderEngine(case.cfg)
+    e.loadWeights(case.weights)
+    env = e.addEnvironmentMap(eng.EnvironmentMap(top_coefficients=case.idx, top_strength=case.strength))
+    fr = eng.FullFrame.from_gbuffer(case.gbuf)
+    e.setFrame(0, fr)
+    e.TCNNPass_p1(0)
+    e.TCNNPass_p2(env, 0, eng.RenderConfig(precision="fp32"))
+    full = e.computeFinalPixelColors(0).cpu().numpy().view(np.uint32)
+    ind = e.computeFinalPixelColors(0, "indirect").cpu().numpy().view(np.uint32)
+    e.TCNNSync()
+    assert np.array_equal(full, O.tonemap_srgb(fr.fbPredictedIndirectWithDirect.cpu().numpy()))
+    assert np.array_equal(ind, O.tonemap_srgb(fr.fbPredictedIndirect.cpu().numpy()))
+    with pytest.raises(ValueError):
+        e.computeFinalPixelColors(0, "direct")
+    e.close()

@@ -211,3 +211,54 @@ def test_embedding_gather_matches_reference_ptwise_mlt():
     out = O.ref_ptwise_mlt(enc_fm, case.weights.wve_enc.ravel(), case.idx)
     mine = enc[:, None, :] * case.weights.wve_enc[:, case.idx].T[None]   # [n, 64, D] float32
     assert np.array_equal(out.T.reshape(n, 64, D), mine.astype(np.float32))
+
+
+# ---------------------------------------------------------------- final-colour pass (tonemap)
+
+def test_powf_series_matches_double_pow():
+    """The series x^(1/2.4) rounds to the float nearest the float64 power (tie cases aside)."""
+    g = np.random.default_rng(5)
+    x = np.concatenate([g.uniform(0, 4, 4000), 10.0 ** g.uniform(-8, 3, 4000)]).astype(np.float32)
+    y = np.float32(1.0) / np.float32(2.4)
+    got = O.powf_series(x, y)
+    ref = np.power(x.astype(np.float64), float(y)).astype(np.float32)
+    ulps = np.abs(got.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64))
+    assert ulps.max() <= 1 and np.mean(ulps == 0) > 0.999
+
+
+def test_tonemap_known_answers_and_edges():
+    x = np.array([0, 0.5, 1, 1e-3, 0.18, 2.0, -1, np.nan, np.inf, -np.inf, 1e-8, 3e38], np.float32)
+    src = np.stack([x, x, x, np.ones_like(x)], 1)
+    t = O.tonemap_srgb(src)
+    r = t & 255
+    assert list(r) == [0, 188, 255, 1, 118, 255, 0, 0, 255, 0, 0, 255]
+    assert np.all((t >> 24) == 255)
+    assert np.all(((t >> 8) & 255) == r) and np.all(((t >> 16) & 255) == r)
+
+
+def test_tonemap_against_float64_formula():
+    """Bytes equal floor(255.9 * clamp(1.055 (x + 1e-6)^(1/2.4) - 0.055)) evaluated in float64,
+    except where that value lies within float rounding of an integer."""
+    g = np.random.default_rng(6)
+    x = np.concatenate([g.uniform(0, 1.2, 20000), 10.0 ** g.uniform(-6, 1, 20000)]).astype(np.float32)
+    src = np.stack([x, np.roll(x, 1), np.roll(x, 2), np.zeros_like(x)], 1)
+    got = O.tonemap_srgb(src)
+    for c in range(3):
+        xc = src[:, c].astype(np.float64)
+        f = np.clip(1.055 * np.power(xc + np.float64(np.float32(1e-6)), 1 / 2.4) - 0.055, 0, 1) * 255.9
+        want = np.floor(f).astype(np.int64)
+        byte = (got >> (8 * c)) & 255
+        near = np.abs(f - np.round(f)) < 1e-4
+        assert np.array_equal(byte[~near], want[~near])
+
+
+def test_srgb_step_table_equals_formula_near_every_step():
+    """The final-colour kernel maps a channel to the number of step thresholds at or below it;
+    around every threshold (+-4096 ulps) that count equals the direct formula."""
+    t = O.srgb_thresholds()
+    assert np.all(np.diff(t[1:]) > 0) and t[1] > 0
+    assert O.srgb_threshold_mismatches(t, 4096) == 0
+    # between thresholds the byte is constant: spot-check the midpoints
+    mid = ((t[1:-1].view(np.uint32).astype(np.uint64) + t[2:].view(np.uint32)) // 2).astype(np.uint32).view(np.float32)
+    src = np.stack([mid, mid, mid, mid], 1)
+    assert np.array_equal(O.tonemap_srgb(src) & 255, np.arange(1, 255, dtype=np.uint32))
