@@ -224,6 +224,23 @@ NWPRT_API nwprt_status nwprt_env_rotate(const float* src, int S, const float* R,
  * packed r | g << 8 | b << 16 | 255 << 24.  src: n_px float4 (16-byte aligned), dst: n_px
  * uint32, both device memory. */
 NWPRT_API nwprt_status nwprt_tonemap_srgb(const float* src, int64_t n_px, uint32_t* dst, void* stream);
+/* SH shading of mesh vertices -- the SH path's closest-hit program without the ray tracer
+ * (Renderer/device_functions/devicePrograms.cu:427-486): for every vertex v,
+ *   light[k] = sum_j T[v][k][j] L[j]  (j ascending),  out[v] = | sum_k light[k] * brdf[v][k] |
+ * per RGB channel (k ascending).  T: [V][n][n] transfer matrices (the reference's T_matrix,
+ * RenderEngine.cpp:410-448), brdf_sh: [V][n][3] the BRDF projected on the SH basis (sampled
+ * from the material in the reference, devicePrograms.cu:448-474), L: [n][3] env SH,
+ * out: [V][3]; n = (degree + 1)^2 <= 81.  All device memory. */
+NWPRT_API nwprt_status nwprt_sh_vertex_radiance(const float* T, const float* brdf_sh, const float* L,
+                                                int64_t n_vertices, int n_coeffs, float* out, void* stream);
+/* Pixel colours from their triangle's vertex colours (devicePrograms.cu:488-490):
+ * out[p] = ((1 - u - v) c[i0] + u c[i1] + v c[i2], 1), evaluated as
+ * fma(v, c2, fma(u, c1, (1 - u - v) c0)).  tri: [P][3] int32 vertex indices, uv: [P][2]
+ * barycentrics, out: [P] float4 (16-byte aligned).  An index outside [0, n_vertices) yields
+ * (0, 0, 0, 1) and is reported by nwprt_sync. */
+NWPRT_API nwprt_status nwprt_sh_interpolate(nwprt_ctx* ctx, const float* vertex_rgb, int64_t n_vertices,
+                                            const int32_t* tri, const float* uv, int64_t n_px, float* out,
+                                            void* stream);
 /* SH projection (order 8, 81 coefficients) of a cubemap [6][S][S][3] -> L[81][3]
  * (the env SH the reference loads from sh/<name>.npy, EnvironmentMap.cpp:70-77).
  * `workspace` must hold nwprt_sh_project_workspace_size(S) bytes of device memory. */

@@ -23,7 +23,8 @@ EXPORTS = (
     "nwprt_env_from_faces", "nwprt_env_from_wavelets", "nwprt_env_get_wavelets", "nwprt_env_release",
     "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_relight_ranges",
     "nwprt_calibrate_fp8", "nwprt_get_fp8_calibration", "nwprt_sync",
-    "nwprt_haar_topk", "nwprt_env_rotate", "nwprt_tonemap_srgb",
+    "nwprt_haar_topk", "nwprt_env_rotate", "nwprt_tonemap_srgb", "nwprt_sh_vertex_radiance",
+    "nwprt_sh_interpolate",
     "nwprt_sh_project_workspace_size", "nwprt_sh_project", "nwprt_sh_project_static", "nwprt_sh_dot",
 )
 
@@ -103,6 +104,8 @@ def lib():
         "nwprt_sync": (_st, [_vp]),
         "nwprt_env_rotate": (_st, [_vp, _i, _vp, _vp, _vp]),
         "nwprt_tonemap_srgb": (_st, [_vp, C.c_int64, _vp, _vp]),
+        "nwprt_sh_vertex_radiance": (_st, [_vp, _vp, _vp, C.c_int64, _i, _vp, _vp]),
+        "nwprt_sh_interpolate": (_st, [_vp, _vp, C.c_int64, _vp, _vp, C.c_int64, _vp, _vp]),
         "nwprt_haar_topk": (_st, [_vp, _i, _i, _i, _vp, _vp, _vp]),
         "nwprt_sh_project_workspace_size": (C.c_size_t, [_i]),
         "nwprt_sh_project": (_st, [_vp, _i, _vp, _vp, C.c_size_t, _vp]),

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
 SOURCES = ["api.cu", "config.cpp", "haar_topk.cu", "sh.cu", "relight_common.cu", "relight_fp32.cu",
-           "relight_tc.cu", "sh_noalloc.cu", "env_rotate.cu", "tonemap.cu"]
+           "relight_tc.cu", "sh_noalloc.cu", "env_rotate.cu", "tonemap.cu", "sh_vertex.cu"]
 HEADERS = ["nwprt_internal.cuh"]
 
 

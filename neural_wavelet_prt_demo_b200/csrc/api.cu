@@ -682,6 +682,19 @@ nwprt_status nwprt_tonemap_srgb(const float* src, int64_t n_px, uint32_t* dst, v
   return guarded(nullptr, [&] { launch_tonemap_srgb(src, n_px, dst, (cudaStream_t)stream); });
 }
 
+nwprt_status nwprt_sh_vertex_radiance(const float* T, const float* brdf_sh, const float* L, int64_t n_vertices,
+                                      int n_coeffs, float* out, void* stream) {
+  return guarded(nullptr, [&] { launch_sh_vertex(T, brdf_sh, L, n_vertices, n_coeffs, out, (cudaStream_t)stream); });
+}
+
+nwprt_status nwprt_sh_interpolate(nwprt_ctx* ctx, const float* vertex_rgb, int64_t n_vertices, const int32_t* tri,
+                                  const float* uv, int64_t n_px, float* out, void* stream) {
+  return guarded(ctx, [&] {
+    need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
+    launch_sh_interpolate(vertex_rgb, n_vertices, tri, uv, n_px, out, ctx->d_err, (cudaStream_t)stream);
+  });
+}
+
 nwprt_status nwprt_sync(nwprt_ctx* ctx) {
   return guarded(ctx, [&] {
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");

@@ -148,6 +148,12 @@ void pack_fp32_weights(const NetDims& d, const float* op, const float* cn,
 // tonemap.cu
 void launch_tonemap_srgb(const float* src, int64_t n, uint32_t* dst, cudaStream_t st);
 
+// sh_vertex.cu
+void launch_sh_vertex(const float* T, const float* brdf, const float* L, int64_t V, int n, float* out,
+                      cudaStream_t st);
+void launch_sh_interpolate(const float* vc, int64_t V, const int32_t* tri, const float* uv, int64_t P, float* out,
+                           uint32_t* err, cudaStream_t st);
+
 // relight_tc.cu (tcgen05 path: BF16 operands, or FP8 e4m3 with per-layer scales)
 constexpr int kMaxTcLayers = 12;
 // One tensor-core layer of the per-wavelet MLP chain (B operand offsets inside the weight blob).

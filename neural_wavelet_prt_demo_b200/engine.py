@@ -347,6 +347,22 @@ class RenderEngine:
         """tcnn.cu:154-158; also surfaces device-side error reports."""
         self._check(lib().nwprt_sync(self._ctx))
 
+    def shInterpolate(self, vertex_rgb: torch.Tensor, tri: torch.Tensor, uv: torch.Tensor,
+                      out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        """Pixel colours of the SH path from per-vertex colours (devicePrograms.cu:488-490):
+        vertex_rgb [V, 3] float32, tri [P, 3] int32, uv [P, 2] float32 -> [P, 4] (rgb, 1).
+        A triangle index outside the vertex range reads as (0, 0, 0, 1) and is reported by
+        TCNNSync."""
+        if vertex_rgb.dtype != torch.float32 or tri.dtype != torch.int32 or uv.dtype != torch.float32:
+            raise ValueError("vertex_rgb float32 [V, 3], tri int32 [P, 3], uv float32 [P, 2]")
+        P = tri.shape[0]
+        if out is None:
+            out = torch.empty((P, 4), dtype=torch.float32, device=vertex_rgb.device)
+        self._check(lib().nwprt_sh_interpolate(self._ctx, _ptr(vertex_rgb.contiguous()), vertex_rgb.shape[0],
+                                               _ptr(tri.contiguous()), _ptr(uv.contiguous()), P, _ptr(out),
+                                               _stream_ptr(stream)))
+        return out
+
     def computeFinalPixelColors(self, frameID: int, renderingMode: str = "full", stream=None) -> torch.Tensor:
         """RenderEngine::computeFinalPixelColors (toneMap.cu:73-98) for the wavelet path: the
         relit frame (indirect + direct for "full", indirect alone for "indirect") -> packed
@@ -412,6 +428,22 @@ def sh_project(faces: torch.Tensor, stream=None) -> torch.Tensor:
     L = torch.empty((81, 3), dtype=torch.float32, device=faces.device)
     check(lib().nwprt_sh_project(_ptr(faces), S, _ptr(L), _ptr(ws), nbytes, _stream_ptr(stream)))
     return L
+
+
+def sh_vertex_radiance(T: torch.Tensor, brdf: torch.Tensor, L: torch.Tensor, out: Optional[torch.Tensor] = None,
+                       stream=None) -> torch.Tensor:
+    """Per-vertex SH shading (devicePrograms.cu:476-486): T [V, n, n], brdf [V, n, 3], L [n, 3]
+    (float32 CUDA) -> [V, 3] = |sum_k (T L)[k] * brdf[k]|."""
+    for a in (T, brdf, L):
+        if a.dtype != torch.float32 or not a.is_cuda or not a.is_contiguous():
+            raise ValueError("T, brdf and L must be contiguous float32 CUDA tensors")
+    V, n = T.shape[0], T.shape[1]
+    if T.shape != (V, n, n) or brdf.shape != (V, n, 3) or L.shape != (n, 3):
+        raise ValueError("shapes must be T [V, n, n], brdf [V, n, 3], L [n, 3]")
+    if out is None:
+        out = torch.empty((V, 3), dtype=torch.float32, device=T.device)
+    check(lib().nwprt_sh_vertex_radiance(_ptr(T), _ptr(brdf), _ptr(L), V, n, _ptr(out), _stream_ptr(stream)))
+    return out
 
 
 def sh_dot(T: torch.Tensor, L: torch.Tensor, abs_out: bool = True, out: Optional[torch.Tensor] = None,

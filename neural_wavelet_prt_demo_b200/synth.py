@@ -25,6 +25,7 @@ _S_HASH, _S_OP, _S_CN, _S_EMB = 1, 2, 3, 4
 _S_POS, _S_NRM, _S_VIEW, _S_KD, _S_KS, _S_RGH, _S_DIR, _S_FLAG = 10, 11, 12, 13, 14, 15, 16, 17
 _S_ENV = 30
 _S_SHT = 40
+_S_TMAT, _S_BRDF, _S_TRI, _S_UV = 41, 42, 43, 44
 
 
 def rng(seed: int, stream: int) -> np.random.Generator:
@@ -143,3 +144,30 @@ def make_sh_transport(n_px: int, n_coeffs: int = 81, seed: int = 0) -> np.ndarra
         e = min(n_px, s + step)
         out[s:e] = g.standard_normal(size=(e - s, n_coeffs), dtype=np.float32) * scale
     return out
+
+
+def make_sh_mesh(n_vertices: int, n_px: int, n_coeffs: int = 81, seed: int = 0):
+    """Synthetic inputs of the per-vertex SH path: T [V][n][n] ~ N(0,1)/(l_k l_j) (the SH
+    transfer matrix of a diffuse-ish vertex decays with both bands), BRDF SH [V][n][3] ~
+    N(0,1)/l_k^2 scaled by a U(0,1) albedo, and for every pixel a random triangle of
+    vertices plus barycentrics (u, v) uniform on the triangle."""
+    l = np.floor(np.sqrt(np.arange(n_coeffs))).astype(np.float64)
+    l[l == 0] = 1.0
+    inv = (1.0 / l).astype(np.float32)
+    g = rng(seed, _S_TMAT)
+    T = np.empty((n_vertices, n_coeffs, n_coeffs), np.float32)
+    step = max(1, (1 << 22) // (n_coeffs * n_coeffs))
+    for s0 in range(0, n_vertices, step):
+        e = min(n_vertices, s0 + step)
+        T[s0:e] = g.standard_normal(size=(e - s0, n_coeffs, n_coeffs), dtype=np.float32) * inv[None, :, None] * inv[None, None, :]
+    g = rng(seed, _S_BRDF)
+    alb = g.uniform(0, 1, size=(n_vertices, 1, 3)).astype(np.float32)
+    brdf = g.standard_normal(size=(n_vertices, n_coeffs, 3), dtype=np.float32) * (inv * inv)[None, :, None] * alb
+    g = rng(seed, _S_TRI)
+    tri = g.integers(0, n_vertices, size=(n_px, 3), dtype=np.int32)
+    g = rng(seed, _S_UV)
+    a, b = g.uniform(0, 1, size=n_px), g.uniform(0, 1, size=n_px)
+    flip = a + b > 1
+    a[flip], b[flip] = 1 - a[flip], 1 - b[flip]
+    uv = np.stack([a, b], 1).astype(np.float32)
+    return T, brdf, tri, uv

@@ -407,6 +407,47 @@ int64_t orc_srgb_threshold_mismatches(const float* t, int radius) {
   return bad;
 }
 
+/* SH shading of mesh vertices (Renderer/device_functions/devicePrograms.cu:476-486):
+ * light[k] = sum_j T[v][k][j] L[j] accumulated with one fma per term in j order
+ * (lightResponse[k] += T * light_vector[j]), then c = sum_k light[k] * brdf[v][k] in k order
+ * (colorTriangleVertices += lightResponse * brdf), and its absolute value per channel. */
+void orc_sh_vertex_radiance(const float* T, const float* brdf, const float* L, int64_t V, int n, float* out) {
+  for (int64_t v = 0; v < V; ++v) {
+    const float* t = T + v * (int64_t)n * n;
+    const float* b = brdf + v * (int64_t)n * 3;
+    float c[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < n; ++k) {
+      float l[3] = {0.f, 0.f, 0.f};
+      for (int j = 0; j < n; ++j)
+        for (int ch = 0; ch < 3; ++ch) l[ch] = fmaf(t[k * n + j], L[j * 3 + ch], l[ch]);
+      for (int ch = 0; ch < 3; ++ch) c[ch] = fmaf(l[ch], b[k * 3 + ch], c[ch]);
+    }
+    for (int ch = 0; ch < 3; ++ch) out[v * 3 + ch] = fabsf(c[ch]);
+  }
+}
+
+/* Barycentric pixel colour (devicePrograms.cu:488-490): ((1 - u) - v) c0 + u c1 + v c2 as
+ * fma(v, c2, fma(u, c1, w c0)); output float4 (rgb, 1).  Returns the number of pixels whose
+ * triangle named a vertex outside [0, V) (those read (0, 0, 0, 1)). */
+int64_t orc_sh_interpolate(const float* vc, int64_t V, const int32_t* tri, const float* uv, int64_t P, float* out) {
+  int64_t bad = 0;
+  for (int64_t p = 0; p < P; ++p) {
+    const int32_t i0 = tri[p * 3], i1 = tri[p * 3 + 1], i2 = tri[p * 3 + 2];
+    float* o = out + p * 4;
+    o[3] = 1.f;
+    if (i0 < 0 || i1 < 0 || i2 < 0 || i0 >= V || i1 >= V || i2 >= V) {
+      o[0] = o[1] = o[2] = 0.f;
+      ++bad;
+      continue;
+    }
+    const float u = uv[p * 2], w = uv[p * 2 + 1];
+    const float b0 = (1.f - u) - w;
+    for (int ch = 0; ch < 3; ++ch)
+      o[ch] = fmaf(w, vc[i2 * 3 + ch], fmaf(u, vc[i1 * 3 + ch], b0 * vc[i0 * 3 + ch]));
+  }
+  return bad;
+}
+
 /* The reference's per-pixel 16-float input row (waveletDataCopy,
  * utils_kernels.h:7-49; layout prt_globals.h:4-13):
  * pos(3) normal(3) reflect(3) log(25r+1)/log(26) 2kd-1(3) 2ks-1(3). */

@@ -82,6 +82,8 @@ float orc_logf_series(float x);
 float orc_powf_series(float x, float y);
 void orc_tonemap_srgb(const float* src, int64_t n, uint32_t* dst);
 void orc_srgb_thresholds(float* t256);
+void orc_sh_vertex_radiance(const float* T, const float* brdf, const float* L, int64_t V, int n, float* out);
+int64_t orc_sh_interpolate(const float* vc, int64_t V, const int32_t* tri, const float* uv, int64_t P, float* out);
 int64_t orc_srgb_threshold_mismatches(const float* t256, int radius);
 void orc_remap_f32(const orc_gbuf* g, int64_t px, float row[16]);
 void orc_hash_encode_f32(const orc_net* net, const float* hash, const float pos[3], float* out);

@@ -186,6 +186,29 @@ def srgb_threshold_mismatches(t: np.ndarray, radius: int) -> int:
     return int(f(_p(np.ascontiguousarray(t, np.float32)), C.c_int(radius)))
 
 
+def sh_vertex_radiance(T: np.ndarray, brdf: np.ndarray, L: np.ndarray) -> np.ndarray:
+    """T [V, n, n], brdf [V, n, 3], L [n, 3] -> |sum_k (T L)[k] * brdf[k]| [V, 3]."""
+    T = np.ascontiguousarray(T, np.float32)
+    brdf = np.ascontiguousarray(brdf, np.float32)
+    L = np.ascontiguousarray(L, np.float32)
+    V, n = T.shape[0], T.shape[1]
+    out = np.empty((V, 3), np.float32)
+    lib().orc_sh_vertex_radiance(_p(T), _p(brdf), _p(L), C.c_int64(V), C.c_int(n), _p(out))
+    return out
+
+
+def sh_interpolate(vc: np.ndarray, tri: np.ndarray, uv: np.ndarray):
+    """Vertex colours [V, 3], triangles [P, 3] int32, barycentrics [P, 2] -> ([P, 4], n_bad)."""
+    vc = np.ascontiguousarray(vc, np.float32)
+    tri = np.ascontiguousarray(tri, np.int32)
+    uv = np.ascontiguousarray(uv, np.float32)
+    out = np.empty((tri.shape[0], 4), np.float32)
+    f = lib().orc_sh_interpolate
+    f.restype = C.c_int64
+    bad = f(_p(vc), C.c_int64(vc.shape[0]), _p(tri), _p(uv), C.c_int64(tri.shape[0]), _p(out))
+    return out, int(bad)
+
+
 def sh_eval_f64(d, lmax=8) -> np.ndarray:
     out = np.zeros((lmax + 1) ** 2, np.float64)
     lib().orc_sh_eval_f64(C.c_double(d[0]), C.c_double(d[1]), C.c_double(d[2]), C.c_int(lmax),

@@ -136,3 +136,32 @@ def test_final_pixel_colors_of_a_relit_frame(cuda):
     with pytest.raises(ValueError):
         e.computeFinalPixelColors(0, "direct")
     e.close()
+
+
+@pytest.mark.parametrize("V,n", [(1, 81), (37, 81), (1000, 81), (33, 9), (17, 1), (5, 4)])
+def test_sh_vertex_radiance_bit_exact(cuda, V, n):
+    import torch
+    from neural_wavelet_prt_demo_b200 import synth
+    eng = _engine()
+    T, brdf, _, _ = synth.make_sh_mesh(V, 1, 81, seed=V)
+    T, brdf = T[:, :n, :n].copy(), brdf[:, :n].copy()
+    L = synth.make_sh_transport(3, 81, seed=5).T[:n].copy()
+    got = eng.sh_vertex_radiance(*(torch.from_numpy(a).to(cuda) for a in (T, brdf, L))).cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), O.sh_vertex_radiance(T, brdf, L).view(np.uint32))
+
+
+def test_sh_interpolate_bit_exact_and_bad_index(cuda):
+    import torch
+    from neural_wavelet_prt_demo_b200 import netconfig, synth
+    eng = _engine()
+    T, brdf, tri, uv = synth.make_sh_mesh(64, 50_000, 81, seed=3)
+    L = synth.make_sh_transport(3, 81, seed=5).T.copy()
+    vc = O.sh_vertex_radiance(T, brdf, L)
+    tri[7] = [0, 64, 1]  # out of range
+    e = eng.RenderEngine(netconfig.CONFIG_SMALL)
+    got = e.shInterpolate(*(torch.from_numpy(a).to(cuda) for a in (vc, tri, uv))).cpu().numpy()
+    ref, bad = O.sh_interpolate(vc, tri, uv)
+    assert bad == 1 and np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    with pytest.raises(eng.NwprtError):
+        e.TCNNSync()
+    e.close()

@@ -262,3 +262,30 @@ def test_srgb_step_table_equals_formula_near_every_step():
     mid = ((t[1:-1].view(np.uint32).astype(np.uint64) + t[2:].view(np.uint32)) // 2).astype(np.uint32).view(np.float32)
     src = np.stack([mid, mid, mid, mid], 1)
     assert np.array_equal(O.tonemap_srgb(src) & 255, np.arange(1, 255, dtype=np.uint32))
+
+
+# ---------------------------------------------------------------- per-vertex SH path
+
+def test_sh_vertex_radiance_matches_float64():
+    from neural_wavelet_prt_demo_b200 import synth
+    T, brdf, tri, uv = synth.make_sh_mesh(20, 50, 81, seed=1)
+    L = synth.make_sh_transport(3, 81, seed=2).T.copy()  # [81, 3]
+    got = O.sh_vertex_radiance(T, brdf, L)
+    ref = np.abs(np.einsum("vkj,jc,vkc->vc", T.astype(np.float64), L.astype(np.float64), brdf.astype(np.float64)))
+    assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+    # lower degree: the leading 4 or 9 coefficients
+    for n in (1, 4, 9):
+        g = O.sh_vertex_radiance(T[:, :n, :n].copy(), brdf[:, :n].copy(), L[:n].copy())
+        r = np.abs(np.einsum("vkj,jc,vkc->vc", T[:, :n, :n].astype(np.float64), L[:n].astype(np.float64),
+                             brdf[:, :n].astype(np.float64)))
+        assert np.abs(g - r).max() <= 1e-5 * max(np.abs(r).max(), 1e-30)
+
+
+def test_sh_interpolate_barycentric():
+    vc = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
+    tri = np.array([[0, 1, 2], [0, 1, 2], [2, 1, 0], [0, 1, 5]], np.int32)
+    uv = np.array([[0, 0], [0.25, 0.5], [1, 0], [0.5, 0.5]], np.float32)
+    out, bad = O.sh_interpolate(vc, tri, uv)
+    assert bad == 1
+    assert np.array_equal(out[0], [1, 0, 0, 1]) and np.allclose(out[1], [0.25, 0.25, 0.5, 1])
+    assert np.array_equal(out[2], [0, 1, 0, 1]) and np.array_equal(out[3], [0, 0, 0, 1])
