@@ -95,8 +95,6 @@ struct nwprt_ctx {
   uint32_t* d_err = nullptr;
   float* d_stage = nullptr;
   size_t stage_cap = 0;
-  TcJob* d_jobs = nullptr;
-  int jobs_cap = 0;
 
   ~nwprt_ctx() {
     DeviceGuard g(device);
@@ -108,7 +106,6 @@ struct nwprt_ctx {
     dev_free(d_tc_w8);
     dev_free(d_err);
     dev_free(d_stage);
-    dev_free(d_jobs);
     for (auto& e : envs) free_env_buffers(e);
     for (auto& f : frames) dev_free(f.packed);
   }
@@ -545,19 +542,12 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
                          0, r.px_begin});
   }
   if (jobs.empty()) return;
-  if (ctx->jobs_cap < (int)jobs.size()) {
-    NWPRT_CUDA(cudaDeviceSynchronize());
-    dev_free(ctx->d_jobs);
-    ctx->d_jobs = nullptr;
-    ctx->d_jobs = dev_alloc<TcJob>(jobs.size());
-    ctx->jobs_cap = (int)jobs.size();
-  }
   if (mode == kTcFp8)
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w8, &ctx->fp8_plan, mode, jobs.data(),
-                      (int)jobs.size(), ctx->d_jobs, o.kahan, o.clamp_terms, nullptr, ctx->d_err, st);
+                      (int)jobs.size(), o.kahan, o.clamp_terms, nullptr, ctx->d_err, st);
   else
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, nullptr, mode, jobs.data(), (int)jobs.size(),
-                      ctx->d_jobs, o.kahan, o.clamp_terms, amax, ctx->d_err, st);
+                      o.kahan, o.clamp_terms, amax, ctx->d_err, st);
 }
 
 static void relight_ranges(nwprt_ctx* ctx, const std::vector<RangeReq>& reqs, const nwprt_relight_opts& o,

@@ -203,8 +203,8 @@ struct TcJob {
 // kTcCalibrate also records per-layer activation maxima into amax (uint bits of floats);
 // kTcFp8 uses the FP8 blob and its plan.
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
-                       const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, TcJob* jobs_dev, int kahan,
-                       int clamp, uint32_t* amax, uint32_t* err, cudaStream_t st);
+                       const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, int kahan, int clamp,
+                       uint32_t* amax, uint32_t* err, cudaStream_t st);
 
 }  // namespace nwprt
 

@@ -26,6 +26,7 @@
 // clamped Kahan sum and writes the next wavelet's first-layer operand hash(p) * E_k+1.
 // Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
 // kDevWaitTimeout and the warpgroup unwinds together.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -44,6 +45,10 @@ constexpr int kAcol = 0;                   // A operand columns [0, 32)
 constexpr int kDcol = 64;                  // accumulator columns [64, 128)
 constexpr int kVlastFloats = 3 * 64;
 constexpr uint64_t kWaitNs = 2000000000ull;
+// The job table travels inside the kernel parameters (sm_100 takes up to 32 KB): a launch
+// needs no host->device copy that could queue behind an unrelated bulk transfer.  Larger
+// batches are split into several launches.
+constexpr int kInlineJobs = 256;
 static_assert(kNWG * kTileCols <= kTmemCols, "TMEM budget");
 
 struct TcParams {
@@ -55,7 +60,7 @@ struct TcParams {
   TcLayer layers[kMaxTcLayers];
   int n_layers;
   int enc_dims;  // D, multiple of 16, <= 32
-  const TcJob* jobs;
+  TcJob jobs[kInlineJobs];
   int n_jobs;
   long long total_tiles;
   int kahan, clamp;
@@ -851,13 +856,19 @@ size_t relight_tc_smem_bytes(const NetDims& d) {
 }
 
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
-                       const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, TcJob* jobs_dev, int kahan,
-                       int clamp, uint32_t* amax, uint32_t* err, cudaStream_t st) {
+                       const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, int kahan, int clamp,
+                       uint32_t* amax, uint32_t* err, cudaStream_t st) {
   std::string why;
   if (!plan_supported(d, &why)) fail(NWPRT_UNSUPPORTED, why);
   if (n_jobs <= 0) return;
   if (mode == kTcFp8 && !plan) fail(NWPRT_NOT_READY, "FP8 relight without a calibrated plan");
   if (mode == kTcCalibrate && !amax) fail(NWPRT_INVALID_ARG, "calibration needs an amax buffer");
+  if (n_jobs > kInlineJobs) {
+    for (int j0 = 0; j0 < n_jobs; j0 += kInlineJobs)
+      launch_relight_tc(d, hl, hash, blob_dev, plan, mode, jobs + j0, std::min(kInlineJobs, n_jobs - j0), kahan,
+                        clamp, amax, err, st);
+    return;
+  }
   const TcPlan P = mode == kTcFp8 ? *plan : plan_bf16(d, nullptr, nullptr, nullptr);
   TcParams p{};
   p.hl = hl;
@@ -874,17 +885,15 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.cp_scale = P.cp_scale;
   p.amax = amax;
   p.err = err;
-  // tile prefix over the jobs, then one copy of the job table (stream ordered)
-  std::vector<TcJob> J(jobs, jobs + n_jobs);
+  // tile prefix over the jobs
   long long tiles = 0;
-  for (auto& j : J) {
-    j.tile_begin = tiles;
-    tiles += (j.n_px - j.px_begin + kTile - 1) / kTile;
+  for (int i = 0; i < n_jobs; ++i) {
+    p.jobs[i] = jobs[i];
+    p.jobs[i].tile_begin = tiles;
+    tiles += (jobs[i].n_px - jobs[i].px_begin + kTile - 1) / kTile;
   }
   if (tiles == 0) return;
   p.total_tiles = tiles;
-  p.jobs = jobs_dev;
-  NWPRT_CUDA(cudaMemcpyAsync(jobs_dev, J.data(), sizeof(TcJob) * J.size(), cudaMemcpyHostToDevice, st));
   int dev = 0, sms = 0, max_smem = 0;
   NWPRT_CUDA(cudaGetDevice(&dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
