@@ -363,6 +363,10 @@ def run_ours(args):
                 "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 FMA/clk x 1965 MHz)"}
     roof["kernel_ms"] = kernel_ms
     roof["algorithmic_flops_per_launch"] = flops
+    if precision != "fp32":
+        # the tensor-core plan folds out_prd's linear output layer into cmp_net's first layer
+        op_in_last, op_out = desc.op_layers()[-1]
+        roof["executed_flops_per_eval"] = desc.flops_per_eval() - 2 * op_in_last * op_out
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -4,8 +4,9 @@
 // per pixel p and wavelet k, cp = hash(p) * E[:, idx_k] -> out_prd MLP -> [o || aux]
 // -> cmp_net MLP -> T_k, and sum_k max(L_k * T_k, 0).  Every hidden dense layer of a
 // 128-pixel x 1-wavelet row block is one tcgen05.mma chain (M=128, N<=64, K=16 steps);
-// the final 3-output layer runs in FP32 on the CUDA cores inside the epilogue of the
-// layer before it, straight from the FP32 accumulator.
+// out_prd's linear output layer is folded into cmp_net's first layer on the host (one
+// round trip less per wavelet); the final 3-output layer runs in FP32 on the CUDA cores
+// inside the epilogue of the layer before it, straight from the FP32 accumulator.
 //
 // Design, from measurements on B200: a tcgen05.mma costs >= ~60 cycles whatever N <= 64,
 // so these 64-wide layers are bound by MMA issue at ~53% of the tensor peak; keeping the
@@ -689,24 +690,52 @@ void put_b(std::vector<uint8_t>* blob, size_t off, const float* src, int n, int 
     }
 }
 
-// Layer table of the tensor-core chain: out_prd layers, then cmp_net's hidden layers (the
-// first one with the aux block), the last one marked fin.  Returns for each layer the
-// weight matrix, its [out][in] shape and the column range used.
-struct LayerSrc {
-  const float* w;
-  int n, k_total, col0, kc;
+// Weights of one tensor-core layer: [n][k] row-major, plus [n][16] for the aux block.
+struct LayerMat {
+  int n, k;
   bool relu, aux;
+  std::vector<float> w, waux;
 };
-std::vector<LayerSrc> layer_sources(const NetDims& d, const float* op, const float* cn) {
-  std::vector<LayerSrc> v;
+
+// The tensor-core chain: out_prd's hidden layers; cmp_net's first layer with out_prd's
+// output layer folded in; cmp_net's remaining hidden layers (the last one marked fin by the
+// plan).  out_prd's output layer is linear (prt_network.h:49-53: no output activation) and
+// feeds cmp_net's first layer directly (prt_network.h:116-131), so
+//   relu(Wc [Wo h ; aux]) = relu((Wc[:, :m] Wo) h + Wc[:, m:] aux)        (m = op_out)
+// exactly; the product Wc[:, :m] Wo is formed here in double, which saves one layer per
+// wavelet.  With op or cn null only the shapes are filled.
+std::vector<LayerMat> layer_mats(const NetDims& d, const float* op, const float* cn) {
+  const bool fill = op && cn;
+  std::vector<LayerMat> v;
   const float* w = op;
-  for (int i = 0; i < d.op_nl; ++i) {
-    v.push_back({w, d.op_outs[i], d.op_in[i], 0, d.op_in[i], i + 1 < d.op_nl, false});
+  for (int i = 0; i + 1 < d.op_nl; ++i) {
+    LayerMat L{d.op_outs[i], d.op_in[i], true, false, {}, {}};
+    if (fill) L.w.assign(w, w + (size_t)d.op_in[i] * d.op_outs[i]);
+    v.push_back(std::move(L));
     if (w) w += (size_t)d.op_in[i] * d.op_outs[i];
   }
-  w = cn;
-  for (int i = 0; i + 1 < d.cn_nl; ++i) {
-    v.push_back({w, d.cn_outs[i], d.cn_in[i], 0, i == 0 ? d.op_out : d.cn_in[i], true, i == 0});
+  const int lo = d.op_nl - 1;  // out_prd's output layer: [op_out][op_in[lo]]
+  const int n0 = d.cn_outs[0], k0 = d.op_in[lo], m = d.op_out, kt = d.cn_in[0];
+  LayerMat F{n0, k0, true, true, {}, {}};
+  if (fill) {
+    const float* wo = w;
+    F.w.resize((size_t)n0 * k0);
+    for (int r = 0; r < n0; ++r)
+      for (int c = 0; c < k0; ++c) {
+        double acc = 0.0;
+        for (int j = 0; j < m; ++j) acc += (double)cn[(size_t)r * kt + j] * (double)wo[(size_t)j * k0 + c];
+        F.w[(size_t)r * k0 + c] = (float)acc;
+      }
+    F.waux.resize((size_t)n0 * 16);
+    for (int r = 0; r < n0; ++r)
+      for (int c = 0; c < 16; ++c) F.waux[(size_t)r * 16 + c] = cn[(size_t)r * kt + m + c];
+  }
+  v.push_back(std::move(F));
+  w = cn ? cn + (size_t)d.cn_in[0] * d.cn_outs[0] : nullptr;
+  for (int i = 1; i + 1 < d.cn_nl; ++i) {
+    LayerMat L{d.cn_outs[i], d.cn_in[i], true, false, {}, {}};
+    if (fill) L.w.assign(w, w + (size_t)d.cn_in[i] * d.cn_outs[i]);
+    v.push_back(std::move(L));
     if (w) w += (size_t)d.cn_in[i] * d.cn_outs[i];
   }
   return v;
@@ -726,25 +755,25 @@ TcPlan make_plan(const NetDims& d, const float* op, const float* cn, int eb, con
   TcPlan P;
   size_t off = 0;
   const bool fill = op && cn;
-  const std::vector<LayerSrc> src = layer_sources(d, op, cn);
+  const std::vector<LayerMat> src = layer_mats(d, op, cn);
   for (size_t li = 0; li < src.size(); ++li) {
-    const LayerSrc& ls = src[li];
+    const LayerMat& ls = src[li];
     TcLayer L{};
-    const int np = pad16(ls.n), kp = eb == 2 ? pad16(ls.kc) : pad32(ls.kc);
+    const int np = pad16(ls.n), kp = eb == 2 ? pad16(ls.k) : pad32(ls.k);
     L.b_off = (uint32_t)off;
     L.b_sbo = (uint32_t)(kp * eb * 8);
     L.k = kp;
     L.n = np;
     L.relu = ls.relu;
     L.scale = 1.f;
-    if (fill) put_b(blob, off, ls.w, ls.n, ls.k_total, ls.col0, ls.kc, np, kp, eb, eb == 2 ? 1.f : g[li]);
+    if (fill) put_b(blob, off, ls.w.data(), ls.n, ls.k, 0, ls.k, np, kp, eb, eb == 2 ? 1.f : g[li]);
     off += (size_t)np * kp * eb;
     off = (off + 127) & ~size_t(127);
     if (ls.aux) {
       // aux block: columns [op_out, op_out + 16) of cmp_net's first layer, BF16
       L.aux = 1;
       L.aux_off = (uint32_t)off;
-      if (fill) put_b(blob, off, ls.w, ls.n, ls.k_total, d.op_out, 16, np, 16, 2, eb == 2 ? 1.f : dscale[li]);
+      if (fill) put_b(blob, off, ls.waux.data(), ls.n, 16, 0, 16, np, 16, 2, eb == 2 ? 1.f : dscale[li]);
       off += (size_t)np * 16 * 2;
       off = (off + 127) & ~size_t(127);
     }
@@ -783,7 +812,7 @@ bool plan_supported(const NetDims& d, std::string* why) {
   if (d.op_out > 64) return no("tensor-core path needs out_prd outputs <= 64");
   if (d.cn_hidden < 1) return no("tensor-core path needs a hidden cmp_net layer");
   if (d.cn_neurons > 64 || pad16(d.cn_neurons) != 64) return no("tensor-core path needs 64-wide cmp_net layers");
-  if (d.op_nl + d.cn_nl - 1 > kMaxTcLayers) return no("too many layers for the tensor-core path");
+  if (d.op_nl + d.cn_nl - 2 > kMaxTcLayers) return no("too many layers for the tensor-core path");
   for (int i = 0; i < d.op_nl; ++i) {
     const int n = pad16(d.op_outs[i]);
     if (n != 32 && n != 64) return no("out_prd widths must pad to 32 or 64");
@@ -802,7 +831,7 @@ bool relight_tc_fp8_supported(const NetDims& d, std::string* why) {
   return true;
 }
 
-int tc_layer_count(const NetDims& d) { return d.op_nl + d.cn_nl - 1; }
+int tc_layer_count(const NetDims& d) { return d.op_nl + d.cn_nl - 2; }
 
 size_t tc_weight_bytes(const NetDims& d) { return plan_bf16(d, nullptr, nullptr, nullptr).blob_bytes; }
 
@@ -823,15 +852,13 @@ void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::ve
 TcPlan pack_tc_weights_fp8(const NetDims& d, const float* op, const float* cn, const float* amax,
                            std::vector<uint8_t>* out) {
   constexpr float kTarget = 240.f, kWmax = 240.f, kWmin = 1.f / 16.f;
-  const std::vector<LayerSrc> src = layer_sources(d, op, cn);
+  const std::vector<LayerMat> src = layer_mats(d, op, cn);
   const int n = (int)src.size();
   std::vector<float> h(n), g(n), epi(n, 1.f), dscale(n);
   for (int l = 0; l < n; ++l) h[l] = amax[l] > 0.f && std::isfinite(amax[l]) ? kTarget / amax[l] : 1.f;
   for (int l = 0; l < n; ++l) {
-    const LayerSrc& ls = src[l];
     float wmax = 0.f;
-    for (int r = 0; r < ls.n; ++r)
-      for (int c = 0; c < ls.kc; ++c) wmax = std::max(wmax, std::fabs(ls.w[(size_t)r * ls.k_total + ls.col0 + c]));
+    for (float x : src[l].w) wmax = std::max(wmax, std::fabs(x));
     if (wmax == 0.f) wmax = 1.f;
     if (l + 1 < n) {
       g[l] = h[l + 1] / h[l];

@@ -66,7 +66,9 @@ def test_fp8_psnr_vs_fp64(cuda, cfg, w, h, K, hs):
     e, env, fr = _rig(case)
     amax = e.calibrateFP8(env, 0)
     desc = netconfig.parse(cfg)
-    n_tc_layers = len(desc.op_layers()) + len(desc.cn_layers()) - 1  # the 3-wide output layer runs in FP32
+    # the 3-wide output layer runs in FP32, and out_prd's linear output layer is folded into
+    # cmp_net's first layer
+    n_tc_layers = len(desc.op_layers()) + len(desc.cn_layers()) - 2
     assert np.all(np.isfinite(amax)) and np.all(amax >= 0) and amax[0] > 0
     assert len(amax) == n_tc_layers + 1
     ind, wd = _run(e, env, fr)
