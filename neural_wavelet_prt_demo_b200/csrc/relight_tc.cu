@@ -17,10 +17,13 @@
 // single tcgen05.st.  Only the weights (B) and the per-tile aux block come from shared
 // memory.
 //
-// Organisation (one persistent CTA per SM): kNWG warpgroups, one 128-pixel tile each,
-// 128 TMEM columns per tile: [0,32) the BF16 A operand (2 values per 32-bit column),
-// [64,128) the FP32 accumulator.  Thread (warp w, lane l) owns tile row 32*(w%4)+l, the
-// TMEM lane it may access.  Per layer: wait on the tile's commit barrier -> tcgen05.ld
+// Organisation (one persistent CTA per SM): kNWG = 5 warpgroups, one 128-pixel tile each,
+// 96 TMEM columns per tile (480 of 512): [0,32) the BF16 A operand (2 values per 32-bit
+// column), [32,96) the FP32 accumulator.  Each tile is an independent chain of MMA ->
+// epilogue round trips, and the kernel is bound by their latency, so five chains beat
+// four (640 threads leave ~96 registers each: the hash features of a tile live in shared
+// memory, and each half of an accumulator is packed and stored back before the next).
+// Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may access.  Per layer: wait on the tile's commit barrier -> tcgen05.ld
 // -> ReLU + cvt.rn.relu.bf16x2 -> tcgen05.st into the A columns -> warpgroup barrier
 // (bar.red.and carrying the "no timeout" vote) -> one elected thread issues the next
 // layer's MMAs and commits them.  The final layer's epilogue forms T_k, does the
@@ -36,14 +39,14 @@
 namespace nwprt {
 namespace {
 
-constexpr int kNWG = 4;                    // warpgroups per CTA, one tile each
+constexpr int kNWG = 5;                    // warpgroups per CTA, one tile each
 constexpr int kThreads = 128 * kNWG;
 constexpr int kTile = 128;                 // pixels per tile (MMA M)
 constexpr int kAuxBytes = kTile * 16 * 2;  // 128 x 16 bf16 aux operand
 constexpr int kTmemCols = 512;
-constexpr int kTileCols = 128;             // TMEM columns per tile
+constexpr int kTileCols = 96;              // TMEM columns per tile
 constexpr int kAcol = 0;                   // A operand columns [0, 32)
-constexpr int kDcol = 64;                  // accumulator columns [64, 128)
+constexpr int kDcol = 32;                  // accumulator columns [32, 96)
 constexpr int kVlastFloats = 3 * 64;
 constexpr uint64_t kWaitNs = 2000000000ull;
 // The job table travels inside the kernel parameters (sm_100 takes up to 32 KB): a launch
@@ -361,44 +364,45 @@ __device__ __forceinline__ void hash_encode_bf16(const HashLevels& hl, const flo
 // or (FP8) scaled by cp_scale and rounded to E4M3, zero-padded to K = 32.  Calibration
 // records max |hash(p) * E_k| in amax[0].
 template <int DMAX, int MODE>
-__device__ __forceinline__ void store_cp(const uint32_t (&enc)[DMAX / 2], const float* __restrict__ ek,
-                                         uint32_t a_taddr, float cp_scale, uint32_t* amax) {
-  float x[DMAX];
+__device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __restrict__ ek, uint32_t a_taddr,
+                                         float cp_scale, uint32_t* amax) {
+  constexpr int NW = MODE == kTcFp8 ? 8 : DMAX / 2;
+  uint32_t cp[NW];
+  float m = 0.f;
 #pragma unroll
   for (int c = 0; c < DMAX / 8; ++c) {
     const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
     const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
-    const uint32_t h0 = enc[c * 4 + 0], h1 = enc[c * 4 + 1], h2 = enc[c * 4 + 2], h3 = enc[c * 4 + 3];
-    x[c * 8 + 0] = __fmul_rn(bf16_lo(h0), e0.x);
-    x[c * 8 + 1] = __fmul_rn(bf16_hi(h0), e0.y);
-    x[c * 8 + 2] = __fmul_rn(bf16_lo(h1), e0.z);
-    x[c * 8 + 3] = __fmul_rn(bf16_hi(h1), e0.w);
-    x[c * 8 + 4] = __fmul_rn(bf16_lo(h2), e1.x);
-    x[c * 8 + 5] = __fmul_rn(bf16_hi(h2), e1.y);
-    x[c * 8 + 6] = __fmul_rn(bf16_lo(h3), e1.z);
-    x[c * 8 + 7] = __fmul_rn(bf16_hi(h3), e1.w);
+    const uint32_t h0 = enc_s[(c * 4 + 0) * kTile], h1 = enc_s[(c * 4 + 1) * kTile];
+    const uint32_t h2 = enc_s[(c * 4 + 2) * kTile], h3 = enc_s[(c * 4 + 3) * kTile];
+    const float x0 = __fmul_rn(bf16_lo(h0), e0.x), x1 = __fmul_rn(bf16_hi(h0), e0.y);
+    const float x2 = __fmul_rn(bf16_lo(h1), e0.z), x3 = __fmul_rn(bf16_hi(h1), e0.w);
+    const float x4 = __fmul_rn(bf16_lo(h2), e1.x), x5 = __fmul_rn(bf16_hi(h2), e1.y);
+    const float x6 = __fmul_rn(bf16_lo(h3), e1.z), x7 = __fmul_rn(bf16_hi(h3), e1.w);
+    if constexpr (MODE == kTcFp8) {
+      cp[c * 2] = pack_e4m3x4<false>(__fmul_rn(x0, cp_scale), __fmul_rn(x1, cp_scale), __fmul_rn(x2, cp_scale),
+                                     __fmul_rn(x3, cp_scale));
+      cp[c * 2 + 1] = pack_e4m3x4<false>(__fmul_rn(x4, cp_scale), __fmul_rn(x5, cp_scale), __fmul_rn(x6, cp_scale),
+                                         __fmul_rn(x7, cp_scale));
+    } else {
+      cp[c * 4 + 0] = pack_bf16(x0, x1);
+      cp[c * 4 + 1] = pack_bf16(x2, x3);
+      cp[c * 4 + 2] = pack_bf16(x4, x5);
+      cp[c * 4 + 3] = pack_bf16(x6, x7);
+    }
+    if constexpr (MODE == kTcCalibrate)
+      m = fmaxf(m, fmaxf(fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(x2), fabsf(x3))),
+                         fmaxf(fmaxf(fabsf(x4), fabsf(x5)), fmaxf(fabsf(x6), fabsf(x7)))));
   }
   if constexpr (MODE == kTcFp8) {
-    uint32_t cp[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
-      cp[i] = i < DMAX / 4 ? pack_e4m3x4<false>(__fmul_rn(x[4 * i], cp_scale), __fmul_rn(x[4 * i + 1], cp_scale),
-                                                __fmul_rn(x[4 * i + 2], cp_scale), __fmul_rn(x[4 * i + 3], cp_scale))
-                           : 0u;
+    for (int i = DMAX / 4; i < 8; ++i) cp[i] = 0u;
     tmem_st8(a_taddr, cp);
   } else {
-    uint32_t cp[DMAX / 2];
-#pragma unroll
-    for (int i = 0; i < DMAX / 2; ++i) cp[i] = pack_bf16(x[2 * i], x[2 * i + 1]);
     if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
     else tmem_st8(a_taddr, cp);
-    if constexpr (MODE == kTcCalibrate) {
-      float m = 0.f;
-#pragma unroll
-      for (int i = 0; i < DMAX; ++i) m = fmaxf(m, fabsf(x[i]));
-      record_amax(amax, __float_as_uint(m));
-    }
   }
+  if constexpr (MODE == kTcCalibrate) record_amax(amax, __float_as_uint(m));
 }
 
 __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long tile) {
@@ -451,7 +455,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;                                       // weight blob (+ V_last)
   uint8_t* aux = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kNWG][kAuxBytes]
-  TcBarriers* bars = reinterpret_cast<TcBarriers*>(aux + kNWG * kAuxBytes);
+  uint32_t* encs = reinterpret_cast<uint32_t*>(aux + kNWG * kAuxBytes);  // [kNWG][DMAX/2][kTile]
+  TcBarriers* bars = reinterpret_cast<TcBarriers*>(encs + kNWG * (DMAX / 2) * kTile);
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int g = warp >> 2;  // warpgroup
@@ -502,11 +507,14 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     const int K = J.K;
     const long long px = J.px_begin + (t - J.tile_begin) * kTile + row;
     const bool valid = px < J.n_px;
-    uint32_t enc[DMAX / 2];
+    uint32_t* enc_s = encs + g * (DMAX / 2) * kTile + row;  // this pixel's features, stride kTile
     if (valid) {
+      uint32_t enc[DMAX / 2];
       const float4* pr = reinterpret_cast<const float4*>(J.packed) + px * 4;
       const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3);
       hash_encode_bf16<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, enc);
+#pragma unroll
+      for (int i = 0; i < DMAX / 2; ++i) enc_s[i * kTile] = enc[i];
       // aux operand: the 13 remapped G-buffer values followed by ones
       st_shared_v4(aux_row, pack_bf16(r0.w, r1.x), pack_bf16(r1.y, r1.z), pack_bf16(r1.w, r2.x),
                    pack_bf16(r2.y, r2.z));
@@ -514,11 +522,11 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
                    pack_bf16(1.f, 1.f));
     } else {
 #pragma unroll
-      for (int i = 0; i < DMAX / 2; ++i) enc[i] = 0u;
+      for (int i = 0; i < DMAX / 2; ++i) enc_s[i * kTile] = 0u;
       st_shared_v4(aux_row, 0, 0, 0, 0);
       st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
     }
-    store_cp<DMAX, MODE>(enc, J.emb_k, a_taddr, p.cp_scale, p.amax);
+    store_cp<DMAX, MODE>(enc_s, J.emb_k, a_taddr, p.cp_scale, p.amax);
     tmem_wait_st();
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     // hand the first layer to the tensor core
@@ -535,38 +543,36 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
           tc_fence_after();
           uint32_t v[32];
           if (!L.fin && MODE == kTcFp8) {
-            uint32_t a[16];
+            uint32_t a[8];
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
             if (L.relu) pack32_e4m3<true>(v, L.scale, a);
             else pack32_e4m3<false>(v, L.scale, a);
+            tmem_st8(a_taddr, a);
             if (L.n > 32) {
               tmem_ld32(d_taddr + 32u, v);
               tmem_wait_ld();
-              if (L.relu) pack32_e4m3<true>(v, L.scale, a + 8);
-              else pack32_e4m3<false>(v, L.scale, a + 8);
-              tmem_st16(a_taddr, a);
-            } else {
-              tmem_st8(a_taddr, a);
+              if (L.relu) pack32_e4m3<true>(v, L.scale, a);
+              else pack32_e4m3<false>(v, L.scale, a);
+              tmem_st8(a_taddr + 8u, a);
             }
             tmem_wait_st();
           } else if (!L.fin) {
-            uint32_t a[32];
+            uint32_t a[16];
             uint32_t m = 0;
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
             if constexpr (MODE == kTcCalibrate) m = amax32(v, L.relu);
             if (L.relu) pack32<true>(v, a);
             else pack32<false>(v, a);
+            tmem_st16(a_taddr, a);
             if (L.n > 32) {
               tmem_ld32(d_taddr + 32u, v);
               tmem_wait_ld();
               if constexpr (MODE == kTcCalibrate) m = max(m, amax32(v, L.relu));
-              if (L.relu) pack32<true>(v, a + 16);
-              else pack32<false>(v, a + 16);
-              tmem_st32(a_taddr, a);
-            } else {
-              tmem_st16(a_taddr, a);
+              if (L.relu) pack32<true>(v, a);
+              else pack32<false>(v, a);
+              tmem_st16(a_taddr + 16u, a);
             }
             if constexpr (MODE == kTcCalibrate) record_amax(p.amax + l + 1, m);
             tmem_wait_st();
@@ -595,7 +601,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
               s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
             }
             if (k + 1 < K) {
-              store_cp<DMAX, MODE>(enc, J.emb_k + (size_t)(k + 1) * p.enc_dims, a_taddr, p.cp_scale, p.amax);
+              store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims, a_taddr, p.cp_scale, p.amax);
               tmem_wait_st();
             }
           }
@@ -878,8 +884,11 @@ TcPlan pack_tc_weights_fp8(const NetDims& d, const float* op, const float* cn, c
   return P;
 }
 
+size_t enc_smem_bytes(const NetDims& d) { return (size_t)kNWG * (d.enc_dims() <= 16 ? 8 : 16) * kTile * 4; }
+
 size_t relight_tc_smem_bytes(const NetDims& d) {
-  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + sizeof(TcBarriers);
+  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + enc_smem_bytes(d) +
+         sizeof(TcBarriers);
 }
 
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
@@ -925,7 +934,8 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   NWPRT_CUDA(cudaGetDevice(&dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const size_t smem = ((P.blob_bytes + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + sizeof(TcBarriers);
+  const size_t smem = ((P.blob_bytes + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + enc_smem_bytes(d) +
+                      sizeof(TcBarriers);
   if (smem > (size_t)max_smem) fail(NWPRT_UNSUPPORTED, "tensor-core relight: shared memory budget exceeded");
   const long long groups = (tiles + kNWG - 1) / kNWG;
   const int grid = (int)(groups < sms ? groups : sms);
