@@ -156,3 +156,24 @@ def test_rejection_timeout_and_error_paths(rig):
     one = serve.request_bytes(frames[2].width * frames[2].height, 300, 64, 32)
     stats = serve.RelightServer(e, frames, base, budget_bytes=one, quantum_ms=0.2, max_queue_s=0.0).run(reqs)
     assert stats["timeout"] >= 1 and stats["done"] >= 1 and stats["done"] + stats["timeout"] == 5
+
+
+def test_more_ranges_than_one_launch_carries(rig):
+    """A batch of more requests than one launch's job table (256) is split into several
+    launches; the pieces still compose to the whole-frame relight bit for bit."""
+    import torch
+    e, frames, base = rig
+    eng = _eng()
+    fr = frames[2]
+    n = fr.width * fr.height                      # 128 x 128 = 16384 px
+    env = e.addEnvironmentFaces(base[0], 64)
+    whole, whole2 = torch.empty((n, 4), device="cuda"), torch.empty((n, 4), device="cuda")
+    e.relightRanges([(env, 2, whole, whole2, 0, n)], eng.RenderConfig(precision="bf16"))
+    cuts = list(range(0, n, 48)) + [n]            # 342 ranges, most not tile-aligned
+    out, out2 = torch.zeros((n, 4), device="cuda"), torch.zeros((n, 4), device="cuda")
+    e.relightRanges([(env, 2, out, out2, cuts[i], cuts[i + 1]) for i in range(len(cuts) - 1)],
+                    eng.RenderConfig(precision="bf16"))
+    e.TCNNSync()
+    assert len(cuts) - 1 > 256
+    assert torch.equal(out, whole) and torch.equal(out2, whole2)
+    e.releaseEnvironmentMap(env)
