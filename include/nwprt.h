@@ -207,7 +207,7 @@ NWPRT_API nwprt_status nwprt_sync(nwprt_ctx* ctx);
 
 /* ---------------------------------------------------------------- kernels without a context */
 /* Haar + top-K of `n_env` cubemaps [n_env][6][S][S][3] -> idx[n_env][K], strength[n_env][K][3].
- * S a power of two <= 128, 1 <= K <= min(6*S*S, 1024).  Order: |luminance| descending,
+ * S a power of two <= 64 (larger faces: NWPRT_UNSUPPORTED), 1 <= K <= min(6*S*S, 1024).  Order: |luminance| descending,
  * flat index face*S*S + row*S + col ascending. */
 NWPRT_API nwprt_status nwprt_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx,
                              float* strength, void* stream);
