@@ -11,6 +11,8 @@
 
 #include "nwprt_internal.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 using namespace nwprt;
 
 namespace {
@@ -117,6 +119,14 @@ void set_error(const nwprt_ctx* ctx, const std::string& m) {
   g_last_error = m;
   if (ctx) const_cast<nwprt_ctx*>(ctx)->last_error = m;
 }
+
+// NVTX range around an entry point (header-only NVTX3: a no-op unless a profiler is attached).
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 template <class F>
 nwprt_status guarded(const nwprt_ctx* ctx, F&& f) {
@@ -294,6 +304,7 @@ nwprt_status nwprt_get_network_info(const nwprt_ctx* ctx, nwprt_network_info* in
 
 nwprt_status nwprt_load_weights(nwprt_ctx* ctx, const nwprt_weights* w) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_load_weights");
     need(ctx && w, NWPRT_INVALID_ARG, "null argument");
     const NetDims& d = ctx->dims;
     need(w->hash_params && w->out_prd && w->cmp_net && w->wve_enc, NWPRT_INVALID_ARG,
@@ -378,6 +389,7 @@ int nwprt_ready(const nwprt_ctx* ctx) {
 nwprt_status nwprt_env_from_faces(nwprt_ctx* ctx, const float* faces, int on_device, int S, int K,
                                   void* stream, int* env_id) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_env_from_faces");
     need(ctx && faces && env_id, NWPRT_INVALID_ARG, "null argument");
     need(S == ctx->dims.face_size, NWPRT_INVALID_ARG,
          "cubemap face size must equal the network's wve_enc.face_size");
@@ -413,6 +425,7 @@ nwprt_status nwprt_env_from_faces(nwprt_ctx* ctx, const float* faces, int on_dev
 nwprt_status nwprt_env_from_wavelets(nwprt_ctx* ctx, const int32_t* idx, const float* strength,
                                      int K, int on_device, void* stream, int* env_id) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_env_from_wavelets");
     need(ctx && idx && strength && env_id, NWPRT_INVALID_ARG, "null argument");
     need(K >= 1 && K <= (1 << 20), NWPRT_INVALID_ARG, "K out of range");
     cudaStream_t st = (cudaStream_t)stream;
@@ -456,6 +469,7 @@ nwprt_status nwprt_env_release(nwprt_ctx* ctx, int env_id) {
 
 nwprt_status nwprt_prepare(nwprt_ctx* ctx, int frame_id, const nwprt_gbuffer* g, void* stream) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_prepare");
     need(ctx && g, NWPRT_INVALID_ARG, "null argument");
     need(frame_id >= 0 && frame_id < NWPRT_MAX_FRAMES, NWPRT_INVALID_ARG, "frame id out of range");
     need(g->width >= 0 && g->height >= 0 && (int64_t)g->width * g->height <= (1LL << 31),
@@ -564,6 +578,7 @@ static void relight_ranges(nwprt_ctx* ctx, const std::vector<RangeReq>& reqs, co
 nwprt_status nwprt_relight(nwprt_ctx* ctx, int env_id, int frame_id, const nwprt_relight_opts* opts,
                            float* indirect, float* with_direct, void* stream) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_relight");
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
     const nwprt_relight_opts o = opts ? *opts : default_opts();
     relight_ranges(ctx, {RangeReq{env_id, frame_id, indirect, with_direct, 0, 0}}, o, (cudaStream_t)stream);
@@ -573,6 +588,7 @@ nwprt_status nwprt_relight(nwprt_ctx* ctx, int env_id, int frame_id, const nwprt
 nwprt_status nwprt_relight_batch(nwprt_ctx* ctx, const nwprt_request* reqs, int n_reqs,
                                  const nwprt_relight_opts* opts, void* stream) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_relight_batch");
     need(ctx && (reqs || n_reqs == 0) && n_reqs >= 0, NWPRT_INVALID_ARG, "bad request list");
     const nwprt_relight_opts o = opts ? *opts : default_opts();
     std::vector<RangeReq> v;
@@ -586,6 +602,7 @@ nwprt_status nwprt_relight_batch(nwprt_ctx* ctx, const nwprt_request* reqs, int 
 nwprt_status nwprt_relight_ranges(nwprt_ctx* ctx, const nwprt_range_request* reqs, int n_reqs,
                                   const nwprt_relight_opts* opts, void* stream) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_relight_ranges");
     need(ctx && (reqs || n_reqs == 0) && n_reqs >= 0, NWPRT_INVALID_ARG, "bad request list");
     const nwprt_relight_opts o = opts ? *opts : default_opts();
     std::vector<RangeReq> v;
@@ -600,6 +617,7 @@ nwprt_status nwprt_relight_ranges(nwprt_ctx* ctx, const nwprt_range_request* req
 nwprt_status nwprt_calibrate_fp8(nwprt_ctx* ctx, int env_id, int frame_id, int64_t px_begin, int64_t px_end,
                                 void* stream) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_calibrate_fp8");
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
     need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
     std::string why;
@@ -680,6 +698,7 @@ nwprt_status nwprt_sh_vertex_radiance(const float* T, const float* brdf_sh, cons
 nwprt_status nwprt_sh_interpolate(nwprt_ctx* ctx, const float* vertex_rgb, int64_t n_vertices, const int32_t* tri,
                                   const float* uv, int64_t n_px, float* out, void* stream) {
   return guarded(ctx, [&] {
+    TraceRange trace("nwprt_sh_interpolate");
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
     launch_sh_interpolate(vertex_rgb, n_vertices, tri, uv, n_px, out, ctx->d_err, (cudaStream_t)stream);
   });
