@@ -15,8 +15,17 @@ the request's first quantum.  The reference renders one frame at a time behind a
 ping-pong (Renderer/OutputVisualizer.cpp:61-126); this generalises that overlap to many
 concurrent requests.
 
-``plan_quantum`` / ``Admission`` are pure host logic (tested on CPU); ``RelightServer``
-drives the GPU.
+Failures stay with the request that caused them.  A request with malformed fields (no such
+frame, K out of range, faces of the wrong shape, a non-finite rotation) is refused at
+admission with status "error"; so is one whose set-up raises (an allocation failure, for
+instance).  If a quantum's launch fails, its ranges are relaunched one request at a time and
+only the requests that still fail are ended.  An optional ``fault`` hook injects such
+failures on the host for testing: it is called with (request, stage) at "arrive" (return
+"drop" to lose the request in transit: status "dropped"), "admit" and "launch" (raise to
+fail the request there).  No failure is ever injected on the GPU.
+
+``plan_quantum`` / ``Admission`` / ``validate_request`` are pure host logic (tested on CPU);
+``RelightServer`` drives the GPU.
 """
 from __future__ import annotations
 
@@ -24,7 +33,7 @@ import math
 import time
 from collections import deque
 from dataclasses import dataclass, field
-from typing import Deque, Dict, List, Optional, Sequence, Tuple
+from typing import Callable, Deque, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -47,7 +56,7 @@ class Request:
     # filled by the server (max_queue_s: longest a request may wait for admission)
     n_px: int = 0
     next_px: int = 0
-    status: str = "pending"   # pending -> queued -> active -> done | rejected | timeout | error
+    status: str = "pending"   # pending -> queued -> active -> done | rejected | timeout | error | dropped
     t_admit: float = math.nan
     t_done: float = math.nan
     env_id: int = -1
@@ -61,6 +70,27 @@ class Request:
     @property
     def latency(self) -> float:
         return self.t_done - self.arrival
+
+
+def validate_request(r: Request, n_res: int, face_size: int, n_base: int) -> None:
+    """Raises ValueError when the request cannot be served as given."""
+    if not math.isfinite(r.arrival):
+        raise ValueError(f"request {r.rid}: arrival time is not finite")
+    if not 0 <= r.res < n_res:
+        raise ValueError(f"request {r.rid}: no resident frame {r.res}")
+    if not 1 <= r.K <= min(1024, 6 * face_size * face_size):
+        raise ValueError(f"request {r.rid}: K={r.K} outside [1, {min(1024, 6 * face_size * face_size)}]")
+    if r.env_kind == "new":
+        if r.faces is None or np.shape(r.faces) != (6, face_size, face_size, 3):
+            raise ValueError(f"request {r.rid}: env faces must be [6, {face_size}, {face_size}, 3]")
+    elif r.env_kind == "rot":
+        if not 0 <= r.base_env < n_base:
+            raise ValueError(f"request {r.rid}: no resident env map {r.base_env}")
+        R = None if r.R is None else np.asarray(r.R, np.float64)
+        if R is None or R.shape != (3, 3) or not np.all(np.isfinite(R)):
+            raise ValueError(f"request {r.rid}: rotation must be a finite 3x3 matrix")
+    else:
+        raise ValueError(f"request {r.rid}: unknown env kind {r.env_kind!r}")
 
 
 def request_bytes(n_px: int, K: int, face_size: int, enc_dims: int) -> int:
@@ -157,7 +187,8 @@ class RelightServer:
 
     def __init__(self, engine, frames, base_faces, precision: str = "bf16", budget_bytes: int = 150 << 30,
                  quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
-                 max_in_flight: int = 2, keep_outputs: bool = False):
+                 max_in_flight: int = 2, keep_outputs: bool = False,
+                 fault: Optional[Callable[[Request, str], Optional[str]]] = None):
         import torch
         self.torch = torch
         self.e = engine
@@ -170,6 +201,7 @@ class RelightServer:
         self.max_queue_s = max_queue_s
         self.max_in_flight = max_in_flight
         self.keep_outputs = keep_outputs
+        self.fault = fault
         self.stream = torch.cuda.current_stream()
         info = engine.networkInfo()
         self.face_size, self.enc_dims = info.face_size, info.enc_dims
@@ -192,6 +224,35 @@ class RelightServer:
         r.env_id = self.e.addEnvironmentFaces(faces, r.K)
         r.outputs = (ind, wd, faces)
 
+    def _end_failed(self, r: Request, t: float) -> None:
+        """Ends a request that failed after admission: returns its budget and env table."""
+        r.status, r.t_done = "error", t
+        if r.bytes_held:
+            self.adm.give(r.bytes_held)
+            r.bytes_held = 0
+        if r.env_id >= 0:
+            try:
+                self.e.releaseEnvironmentMap(r.env_id)
+            except Exception:
+                pass  # an env id the request itself corrupted
+            r.env_id = -1
+        r.outputs = ()
+
+    def _launch(self, ranges_by_req: List[Tuple[Request, Tuple]]) -> List[Request]:
+        """One relight launch for the quantum; if it fails, one launch per request.  Returns
+        the requests whose ranges failed even alone."""
+        try:
+            self.e.relightRanges([rg for _, rg in ranges_by_req], self.cfg)
+            return []
+        except Exception:
+            failed = []
+            for r, rg in ranges_by_req:
+                try:
+                    self.e.relightRanges([rg], self.cfg)
+                except Exception:
+                    failed.append(r)
+            return failed
+
     def run(self, requests: List[Request], realtime: bool = True) -> Dict:
         torch = self.torch
         pending: Deque[Request] = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
@@ -199,8 +260,8 @@ class RelightServer:
         active: List[Request] = []
         in_flight: Deque[Tuple] = deque()
         for r in requests:
-            fr = self.frames[r.res]
-            r.n_px = fr.width * fr.height
+            ok = isinstance(r.res, (int, np.integer)) and 0 <= r.res < len(self.frames)
+            r.n_px = self.frames[r.res].width * self.frames[r.res].height if ok else 0
             r.next_px = 0
             r.status = "pending"
         t0 = time.perf_counter()
@@ -211,11 +272,22 @@ class RelightServer:
             t = now() if realtime else math.inf
             while pending and pending[0].arrival <= t:
                 r = pending.popleft()
+                if self.fault is not None and self.fault(r, "arrive") == "drop":
+                    r.status, r.t_done = "dropped", now()
+                    finished += 1
+                    continue
                 r.status = "queued"
                 queue.append(r)
             # admission (FCFS under the byte budget; over-budget and stale requests are refused)
             while queue:
                 r = queue[0]
+                try:
+                    validate_request(r, len(self.frames), self.face_size, len(self.base_faces))
+                except ValueError:
+                    queue.popleft()
+                    r.status, r.t_done = "error", now()
+                    finished += 1
+                    continue
                 nbytes = request_bytes(r.n_px, r.K, self.face_size, self.enc_dims)
                 if nbytes > self.adm.budget:
                     queue.popleft()
@@ -231,9 +303,11 @@ class RelightServer:
                     break
                 queue.popleft()
                 try:
+                    if self.fault is not None:
+                        self.fault(r, "admit")
                     self._prepare(r)
                 except Exception:
-                    r.status, r.t_done = "error", now()
+                    self._end_failed(r, now())
                     finished += 1
                     continue
                 self.adm.take(nbytes)
@@ -243,14 +317,32 @@ class RelightServer:
             self.max_active = max(self.max_active, len(active))
             if active and len(in_flight) < self.max_in_flight:
                 plan = plan_quantum(active, self.quantum)
-                ranges = []
+                launch = []
                 for r, b, e in plan:
-                    ranges.append((r.env_id, r.res, r.outputs[0], r.outputs[1], b, e))
-                    r.next_px = e
-                self.e.relightRanges(ranges, self.cfg)
+                    try:
+                        if self.fault is not None:
+                            self.fault(r, "launch")
+                    except Exception:
+                        active.remove(r)
+                        self._end_failed(r, now())
+                        finished += 1
+                        continue
+                    launch.append((r, (r.env_id, r.res, r.outputs[0], r.outputs[1], b, e), e))
+                if not launch:
+                    continue
+                torch.cuda.nvtx.range_push(f"quantum {self.quanta}: {len(launch)} requests")
+                failed = self._launch([(r, rg) for r, rg, _ in launch])
+                torch.cuda.nvtx.range_pop()
+                for r in failed:
+                    active.remove(r)
+                    self._end_failed(r, now())
+                    finished += 1
+                for r, _, e in launch:
+                    if r.status == "active":
+                        r.next_px = e
                 ev = torch.cuda.Event()
                 ev.record(self.stream)
-                done_now = [r for r, _, _ in plan if r.next_px >= r.n_px]
+                done_now = [r for r, _, _ in launch if r.status == "active" and r.next_px >= r.n_px]
                 for r in done_now:
                     active.remove(r)
                 in_flight.append((ev, done_now))
@@ -290,6 +382,7 @@ def summarize(requests: Sequence[Request], makespan: float) -> Dict:
         "rejected": sum(r.status == "rejected" for r in requests),
         "timeout": sum(r.status == "timeout" for r in requests),
         "error": sum(r.status == "error" for r in requests),
+        "dropped": sum(r.status == "dropped" for r in requests),
         "makespan_s": makespan,
         "evals_per_s": evals / makespan if makespan > 0 else math.nan,
         "p50_ms": percentile(lat, 50),

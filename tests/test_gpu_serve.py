@@ -177,3 +177,38 @@ def test_more_ranges_than_one_launch_carries(rig):
     assert len(cuts) - 1 > 256
     assert torch.equal(out, whole) and torch.equal(out2, whole2)
     e.releaseEnvironmentMap(env)
+
+
+def test_injected_faults_stay_with_their_requests(rig):
+    """Host-side fault injection: a request lost in transit, one malformed request, an
+    allocation failure at set-up, a failure detected at launch, and a request whose env id
+    is corrupted so that its quantum's launch raises.  Each ends alone; every other request
+    is served and equals its solo result, and the whole budget is returned."""
+    import torch
+    e, frames, base = rig
+    reqs = _requests(10, seed=9, spacing=0.0)
+    reqs[2].K = 0                                   # malformed: refused at admission
+
+    def fault(r, stage):
+        if stage == "arrive" and r.rid == 1:
+            return "drop"
+        if stage == "admit" and r.rid == 3:
+            raise MemoryError("simulated allocation failure")
+        if stage == "launch" and r.rid == 4:
+            raise RuntimeError("simulated corrupt request")
+        if stage == "launch" and r.rid == 6:
+            r.env_id = 10_000                       # the batched launch fails; isolation ends r 6 only
+        return None
+
+    srv = serve.RelightServer(e, frames, base, quantum_ms=0.05, est_evals_per_s=9e9, keep_outputs=True,
+                              fault=fault)
+    stats = srv.run(reqs)
+    status = {r.rid: r.status for r in reqs}
+    assert status[1] == "dropped" and status[2] == "error" and status[3] == "error"
+    assert status[4] == "error" and status[6] == "error"
+    assert stats["dropped"] == 1 and stats["error"] == 4 and stats["done"] == 5
+    assert srv.adm.used == 0
+    for r in reqs:
+        if r.status == "done":
+            ind, wd = _solo(e, frames, base, r)
+            assert torch.equal(r.outputs[0], ind) and torch.equal(r.outputs[1], wd), r.rid

@@ -76,3 +76,24 @@ def test_summary_percentiles():
         r.status, r.t_done, r.n_px = "done", (i + 1) / 1000.0, 1
     s = serve.summarize(reqs, 1.0)
     assert s["done"] == 100 and abs(s["p50_ms"] - 50.5) < 1e-9 and abs(s["p99_ms"] - 99.01) < 1e-9
+
+
+def test_validate_request_refuses_malformed_fields():
+    g = np.random.default_rng(0)
+    good_new = serve.Request(0, 0.0, 1, 64, "new", faces=np.zeros((6, 8, 8, 3), np.float32))
+    good_rot = serve.Request(1, 0.0, 0, 300, "rot", base_env=2, R=serve.random_rotation(g))
+    for r in (good_new, good_rot):
+        serve.validate_request(r, n_res=2, face_size=8, n_base=3)
+    bad = [
+        serve.Request(2, 0.0, 2, 64, "rot", base_env=0, R=np.eye(3)),            # no such frame
+        serve.Request(3, 0.0, 0, 0, "rot", base_env=0, R=np.eye(3)),             # K = 0
+        serve.Request(4, 0.0, 0, 385, "rot", base_env=0, R=np.eye(3)),           # K > 6*8*8
+        serve.Request(5, 0.0, 0, 64, "new", faces=np.zeros((6, 4, 4, 3))),       # wrong face size
+        serve.Request(6, 0.0, 0, 64, "rot", base_env=3, R=np.eye(3)),            # no such env map
+        serve.Request(7, 0.0, 0, 64, "rot", base_env=0, R=np.full((3, 3), np.nan)),
+        serve.Request(8, 0.0, 0, 64, "blur"),
+        serve.Request(9, math.nan, 0, 64, "rot", base_env=0, R=np.eye(3)),
+    ]
+    for r in bad:
+        with pytest.raises(ValueError):
+            serve.validate_request(r, n_res=2, face_size=8, n_base=3)
