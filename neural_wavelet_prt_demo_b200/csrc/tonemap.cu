@@ -92,7 +92,7 @@ void launch_tonemap_srgb(const float* src, int64_t n, uint32_t* dst, cudaStream_
   NWPRT_CUDA(cudaGetDevice(&dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int64_t blocks = (n + kPix * 256 - 1) / (kPix * 256);
-  const int64_t cap = (int64_t)sms * 8;
+  const int64_t cap = (int64_t)sms * 64;  // measured: 8 -> 64 blocks per SM took 16 frames from 193 to 164 us
   tonemap_srgb_kernel<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(
       table(), reinterpret_cast<const float4*>(src), n, dst);
   NWPRT_CUDA(cudaGetLastError());
