@@ -1,12 +1,20 @@
 """Benchmark of the neural wavelet PRT relight pass (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision auto|bf16|fp32] [--workload relight1080|sh1080]
+                    [--precision auto|bf16|fp32]
+                    [--workload relight1080|sh1080|shvertex|haar|tonemap|serve|sweep]
 
 Default workload: relight of a 1920x1080 synthetic G-buffer with K=300 wavelets of a
 6x64x64 env map through the 16-level hash grid + 64-wide MLP network (FP16-rounded
 random-init params).  One step = TCNNPass_p1 + TCNNPass_p2 of one frame.  Metric:
-pixel*wavelet evaluations per second, whole job.
+pixel*wavelet evaluations per second, whole job.  The line also carries the end-to-end
+figure through the public API with host buffers (``e2e``), the plain FP32 drop-in and the
+FP8 form of the same step, the relight kernel's roofline, and the CPU baseline.
+
+Other workloads: ``sh1080`` (SH dot, HBM roofline), ``shvertex`` (per-vertex SH shading +
+interpolation), ``haar`` (Haar + top-K of 1024 env maps), ``tonemap`` (final-colour pass),
+``serve`` (the config-4 serving stream: p50/p99 latency and throughput) and ``sweep`` (the
+config-3 precision sweep against the FP64 oracle).
 
 Multi-GPU (torchrun): every rank relights its own frame (request-level data
 parallelism, no collective on the data path); timing is the max over ranks.
