@@ -195,14 +195,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
       : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
-      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-      NWPRT_W8(0), NWPRT_W8(8), NWPRT_W8(16), NWPRT_W8(24)
-      : "memory");
-}
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
   asm volatile(
@@ -301,19 +293,34 @@ __device__ __forceinline__ void pack32(const uint32_t (&v)[32], uint32_t* out) {
   }
 }
 
-// T += V_last[:, j0:j0+32] relu(h[j0:j0+32]) in FP32 (ascending j).
-__device__ __forceinline__ void final_dot32(const uint32_t (&v)[32], const float* __restrict__ sV, int j0,
-                                            float& t0, float& t1, float& t2) {
+// Two FP32 values in one 64-bit register, for the packed f32x2 arithmetic of sm_100.
+__device__ __forceinline__ unsigned long long pk2(float x, float y) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ void fma2(unsigned long long& acc, unsigned long long a, unsigned long long b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
+__device__ __forceinline__ float sum2(unsigned long long x) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x));
+  return __fadd_rn(lo, hi);
+}
+// T += V_last[:, j0:j0+32] relu(h[j0:j0+32]) in FP32 with packed FMAs: q_c holds the
+// partial sums of channel c over even and odd j, added once at the end (sum2).
+__device__ __forceinline__ void final_dot32x2(const uint32_t (&v)[32], const float* __restrict__ sV, int j0,
+                                              unsigned long long& q0, unsigned long long& q1, unsigned long long& q2) {
 #pragma unroll
   for (int j4 = 0; j4 < 8; ++j4) {
     const float4 a = *reinterpret_cast<const float4*>(sV + 0 * 64 + j0 + 4 * j4);
     const float4 b = *reinterpret_cast<const float4*>(sV + 1 * 64 + j0 + 4 * j4);
     const float4 c = *reinterpret_cast<const float4*>(sV + 2 * 64 + j0 + 4 * j4);
-    const float h0 = fmaxf(__uint_as_float(v[4 * j4 + 0]), 0.f), h1 = fmaxf(__uint_as_float(v[4 * j4 + 1]), 0.f);
-    const float h2 = fmaxf(__uint_as_float(v[4 * j4 + 2]), 0.f), h3 = fmaxf(__uint_as_float(v[4 * j4 + 3]), 0.f);
-    t0 = fmaf(a.x, h0, t0); t0 = fmaf(a.y, h1, t0); t0 = fmaf(a.z, h2, t0); t0 = fmaf(a.w, h3, t0);
-    t1 = fmaf(b.x, h0, t1); t1 = fmaf(b.y, h1, t1); t1 = fmaf(b.z, h2, t1); t1 = fmaf(b.w, h3, t1);
-    t2 = fmaf(c.x, h0, t2); t2 = fmaf(c.y, h1, t2); t2 = fmaf(c.z, h2, t2); t2 = fmaf(c.w, h3, t2);
+    const unsigned long long h01 = pk2(fmaxf(__uint_as_float(v[4 * j4 + 0]), 0.f), fmaxf(__uint_as_float(v[4 * j4 + 1]), 0.f));
+    const unsigned long long h23 = pk2(fmaxf(__uint_as_float(v[4 * j4 + 2]), 0.f), fmaxf(__uint_as_float(v[4 * j4 + 3]), 0.f));
+    fma2(q0, pk2(a.x, a.y), h01); fma2(q0, pk2(a.z, a.w), h23);
+    fma2(q1, pk2(b.x, b.y), h01); fma2(q1, pk2(b.z, b.w), h23);
+    fma2(q2, pk2(c.x, c.y), h01); fma2(q2, pk2(c.z, c.w), h23);
   }
 }
 
@@ -582,11 +589,13 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
             if constexpr (MODE == kTcCalibrate) m = amax32(v, true);
-            final_dot32(v, sV, 0, t0, t1, t2);
+            unsigned long long q0 = 0ull, q1 = 0ull, q2 = 0ull;
+            final_dot32x2(v, sV, 0, q0, q1, q2);
             tmem_ld32(d_taddr + 32u, v);
             tmem_wait_ld();
             if constexpr (MODE == kTcCalibrate) record_amax(p.amax + p.n_layers, max(m, amax32(v, true)));
-            final_dot32(v, sV, 32, t0, t1, t2);
+            final_dot32x2(v, sV, 32, q0, q1, q2);
+            t0 = sum2(q0); t1 = sum2(q1); t2 = sum2(q2);
             const float* Lk = J.strength + (size_t)k * 3;
             float u0 = __fmul_rn(__ldg(Lk + 0), t0);
             float u1 = __fmul_rn(__ldg(Lk + 1), t1);
