@@ -201,6 +201,12 @@ NWPRT_API nwprt_status nwprt_calibrate_fp8(nwprt_ctx* ctx, int env_id, int frame
  * output layer.  Writes min(capacity, n) values and sets *n_values = n. */
 NWPRT_API nwprt_status nwprt_get_fp8_calibration(const nwprt_ctx* ctx, float* amax, int capacity,
                                                  int* n_values);
+/* Diagnostics (no counterpart in the reference): launches one warp that waits, through the
+ * bounded wait every persistent kernel of this library uses, on a barrier that nothing ever
+ * signals.  The wait gives up after timeout_ms (1..2000) and records a timeout, so the next
+ * nwprt_sync returns NWPRT_TIMEOUT and clears it; the context stays usable.  It shows that a
+ * device wait that cannot finish surfaces as a status instead of a hang. */
+NWPRT_API nwprt_status nwprt_selftest_device_wait(nwprt_ctx* ctx, int timeout_ms, void* stream);
 /* Blocks until all work the context issued has finished -- RenderEngine::TCNNSync
  * (tinycudann/tcnn.cu:154-158). */
 NWPRT_API nwprt_status nwprt_sync(nwprt_ctx* ctx);

@@ -22,7 +22,7 @@ EXPORTS = (
     "nwprt_get_network_info", "nwprt_load_weights", "nwprt_load_weights_dir", "nwprt_ready",
     "nwprt_env_from_faces", "nwprt_env_from_wavelets", "nwprt_env_get_wavelets", "nwprt_env_release",
     "nwprt_prepare", "nwprt_relight", "nwprt_relight_batch", "nwprt_relight_ranges",
-    "nwprt_calibrate_fp8", "nwprt_get_fp8_calibration", "nwprt_sync",
+    "nwprt_calibrate_fp8", "nwprt_get_fp8_calibration", "nwprt_selftest_device_wait", "nwprt_sync",
     "nwprt_haar_topk", "nwprt_env_rotate", "nwprt_tonemap_srgb", "nwprt_sh_vertex_radiance",
     "nwprt_sh_interpolate",
     "nwprt_sh_project_workspace_size", "nwprt_sh_project", "nwprt_sh_project_static", "nwprt_sh_dot",
@@ -101,6 +101,7 @@ def lib():
         "nwprt_relight_ranges": (_st, [_vp, C.POINTER(RangeRequest), _i, C.POINTER(RelightOpts), _vp]),
         "nwprt_calibrate_fp8": (_st, [_vp, _i, _i, C.c_int64, C.c_int64, _vp]),
         "nwprt_get_fp8_calibration": (_st, [_vp, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
+        "nwprt_selftest_device_wait": (_st, [_vp, _i, _vp]),
         "nwprt_sync": (_st, [_vp]),
         "nwprt_env_rotate": (_st, [_vp, _i, _vp, _vp, _vp]),
         "nwprt_tonemap_srgb": (_st, [_vp, C.c_int64, _vp, _vp]),

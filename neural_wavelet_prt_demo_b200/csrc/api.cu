@@ -704,6 +704,13 @@ nwprt_status nwprt_sh_interpolate(nwprt_ctx* ctx, const float* vertex_rgb, int64
   });
 }
 
+nwprt_status nwprt_selftest_device_wait(nwprt_ctx* ctx, int timeout_ms, void* stream) {
+  return guarded(ctx, [&] {
+    need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");
+    launch_wait_selftest(timeout_ms, ctx->d_err, (cudaStream_t)stream);
+  });
+}
+
 nwprt_status nwprt_sync(nwprt_ctx* ctx) {
   return guarded(ctx, [&] {
     need(ctx != nullptr, NWPRT_INVALID_ARG, "null context");

@@ -177,6 +177,8 @@ struct TcPlan {
 };
 enum TcMode { kTcBf16 = 0, kTcCalibrate = 1, kTcFp8 = 2 };
 bool relight_tc_supported(const NetDims& d, std::string* why);
+// A bounded device wait that is made to run out (diagnostics of the timeout path).
+void launch_wait_selftest(int timeout_ms, uint32_t* err, cudaStream_t st);
 bool relight_tc_fp8_supported(const NetDims& d, std::string* why);
 size_t tc_weight_bytes(const NetDims& d);
 void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);

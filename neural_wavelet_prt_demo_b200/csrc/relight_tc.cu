@@ -92,14 +92,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
   return done != 0;
 }
 
-// Wait for the phase with `parity`, bounded by kWaitNs of wall time.
-__device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err) {
+// Wait for the phase with `parity`, bounded by limit_ns of wall time (kWaitNs in the kernels).
+__device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err,
+                                             uint64_t limit_ns = kWaitNs) {
   const uint32_t a = smem_u32(bar);
   if (mbar_try(a, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1; it < (1u << 30); ++it) {
     if (mbar_try(a, parity)) return true;
-    if ((it & 255u) == 0 && globaltimer() - t0 > kWaitNs) break;
+    if ((it & 255u) == 0 && globaltimer() - t0 > limit_ns) break;
   }
   atomicCAS(err, 0u, (uint32_t)kDevWaitTimeout);
   return false;
@@ -839,6 +840,26 @@ bool plan_supported(const NetDims& d, std::string* why) {
 }  // namespace
 
 bool relight_tc_supported(const NetDims& d, std::string* why) { return plan_supported(d, why); }
+
+namespace {
+// One warp waits, through the relight kernel's bounded wait, on a barrier that nothing ever
+// arrives on; the wait gives up after limit_ns and records kDevWaitTimeout in err.
+__global__ void wait_selftest_kernel(uint64_t limit_ns, uint32_t* err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  (void)__all_sync(0xffffffffu, wait_bounded(&bar, 0, err, limit_ns));
+}
+}  // namespace
+
+void launch_wait_selftest(int timeout_ms, uint32_t* err, cudaStream_t st) {
+  if (timeout_ms < 1 || timeout_ms > 2000) fail(NWPRT_INVALID_ARG, "wait self-test: timeout_ms must be in [1, 2000]");
+  wait_selftest_kernel<<<1, 32, 0, st>>>((uint64_t)timeout_ms * 1000000ull, err);
+  NWPRT_CUDA(cudaGetLastError());
+}
 
 bool relight_tc_fp8_supported(const NetDims& d, std::string* why) {
   if (!plan_supported(d, why)) return false;

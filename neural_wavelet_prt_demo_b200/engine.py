@@ -343,6 +343,11 @@ class RenderEngine:
         self._check(lib().nwprt_env_release(self._ctx, self.envIds[envMapID]))
         self.envIds[envMapID] = -1
 
+    def selftestDeviceWait(self, timeout_ms: int = 50, stream=None) -> None:
+        """Diagnostics: a device wait that can never finish gives up after timeout_ms and is
+        reported by the next TCNNSync as a TIMEOUT error; the context stays usable."""
+        self._check(lib().nwprt_selftest_device_wait(self._ctx, int(timeout_ms), _stream_ptr(stream)))
+
     def TCNNSync(self) -> None:
         """tcnn.cu:154-158; also surfaces device-side error reports."""
         self._check(lib().nwprt_sync(self._ctx))
