@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
                     help="requests of the stream also served by the plain FP32 serial baseline")
     ap.add_argument("--fp8-steps", type=int, default=5, help="timed steps of the FP8 form (0: skip)")
+    ap.add_argument("--graph-steps", type=int, default=5, help="timed replays of the captured step (0: skip)")
     ap.add_argument("--fp32-steps", type=int, default=2, help="timed steps of the plain FP32 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -319,6 +320,14 @@ def run_ours(args):
            "pipeline": "2 frames; uploads and read-backs on their own streams overlap the other frame's relight",
            "readback_matches_device": ok}
 
+    # ---- the same step replayed from a CUDA graph (TCNNPass_p1 + TCNNPass_p2 captured once)
+    graph = None
+    if args.graph_steps > 0:
+        gr = e.captureRelight(env_id, 0, cfg)
+        msg = timed(gr.replay, args.graph_steps, 2)
+        graph = {"value": world * evals / (msg / 1e3), "unit": "evals/s", "ms_per_step": msg}
+        del gr
+
     # ---- the plain FP32 drop-in path, same workload (for the served/plain ratio)
     plain = None
     if precision != "fp32" and args.fp32_steps > 0:
@@ -395,7 +404,7 @@ def run_ours(args):
                        "l2": f"inputs {h2d / 1e6:.0f} MB/frame vs 126 MB L2 (no flush)",
                        "parallelism": f"request-dp{world}", "step": "TCNNPass_p1 + TCNNPass_p2"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
-            "clocks": clocks, "plain_fp32": plain, "fp8_e4m3": fp8,
+            "clocks": clocks, "plain_fp32": plain, "fp8_e4m3": fp8, "cuda_graph": graph,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -343,6 +343,24 @@ class RenderEngine:
         self._check(lib().nwprt_env_release(self._ctx, self.envIds[envMapID]))
         self.envIds[envMapID] = -1
 
+    def captureRelight(self, envMapID: int, frameID: int, config: Optional[RenderConfig] = None):
+        """TCNNPass_p1 + TCNNPass_p2 of one frame and env map captured into a CUDA graph
+        (torch.cuda.CUDAGraph).  Each replay() relights whatever the frame's G-buffer tensors
+        hold at that moment into its output tensors, with no host work per frame.  One eager
+        pass runs first, so one-time set-up (buffer growth, the env's embedding rows) stays out
+        of the graph.  The frame's tensors, the env map and the weights must stay in place
+        while the graph is used: a weight load, a frame of another size or releasing the env
+        map invalidates it."""
+        config = config or RenderConfig()
+        self.TCNNPass_p1(frameID)
+        self.TCNNPass_p2(envMapID, frameID, config)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="relaxed"):
+            self.TCNNPass_p1(frameID)
+            self.TCNNPass_p2(envMapID, frameID, config)
+        return g
+
     def selftestDeviceWait(self, timeout_ms: int = 50, stream=None) -> None:
         """Diagnostics: a device wait that can never finish gives up after timeout_ms and is
         reported by the next TCNNSync as a TIMEOUT error; the context stays usable."""
