@@ -8,10 +8,12 @@
 // round trip less per wavelet); the final 3-output layer runs in FP32 on the CUDA cores
 // inside the epilogue of the layer before it, straight from the FP32 accumulator.
 //
-// Design, from measurements on B200: a tcgen05.mma costs >= ~60 cycles whatever N <= 64,
-// so these 64-wide layers are bound by MMA issue at ~53% of the tensor peak; keeping the
-// activations in shared memory made the kernel shared-memory-bandwidth bound instead
-// (operand reads + epilogue stores ~266 KB per tile and wavelet).  So activations live
+// Design, from measurements on B200: an M=128 N=64 tcgen05.mma issued back to back from an
+// elected lane of a converged warp takes ~36 cycles (~90% of the tensor peak), and five
+// independent 4-MMA layer chains saturate the pipe; issued from a lone lane of a diverged
+// warp the same MMAs take ~75 cycles, which cost this kernel 23%.  Keeping the activations
+// in shared memory made the kernel shared-memory-bandwidth bound (operand reads + epilogue
+// stores ~266 KB per tile and wavelet).  So activations live
 // in TMEM: the A operand of every layer is read by the MMA straight from tensor memory
 // (the ".kind::f16 [d], [a], b_desc" form), and the epilogue writes it back with a
 // single tcgen05.st.  Only the weights (B) and the per-tile aux block come from shared
@@ -25,7 +27,7 @@
 // memory, and each half of an accumulator is packed and stored back before the next).
 // Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may access.  Per layer: wait on the tile's commit barrier -> tcgen05.ld
 // -> ReLU + cvt.rn.relu.bf16x2 -> tcgen05.st into the A columns -> warpgroup barrier
-// (bar.red.and carrying the "no timeout" vote) -> one elected thread issues the next
+// (bar.red.and carrying the "no timeout" vote) -> an elected lane of warp 0 issues the next
 // layer's MMAs and commits them.  The final layer's epilogue forms T_k, does the
 // clamped Kahan sum and writes the next wavelet's first-layer operand hash(p) * E_k+1.
 // Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
@@ -104,6 +106,19 @@ __device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity, uin
   }
   atomicCAS(err, 0u, (uint32_t)kDevWaitTimeout);
   return false;
+}
+
+// One lane of a converged warp (elect.sync).  Issuing tcgen05.mma from an elected lane of a
+// converged warp is about twice as fast as from a lone lane whose warp has diverged: back to
+// back M=128 N=64 MMAs take ~36 cycles each instead of ~75.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t e;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "elect.sync _|p, 0xffffffff;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(e));
+  return e != 0;
 }
 
 // Warpgroup barrier (named barrier 1+g, 128 threads) that also ANDs a predicate.
@@ -470,7 +485,6 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   const int g = warp >> 2;  // warpgroup
   const int q = warp & 3;   // TMEM lane quarter this warp may access
   const int row = q * 32 + lane;
-  const bool leader = (tid & 127) == 0;
 
   // ---- weights -> shared memory (generic proxy), barriers, TMEM
   for (uint32_t i = tid; i < p.wblob_bytes / 16u; i += kThreads)
@@ -541,7 +555,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     tc_fence_before();
     fence_proxy_async_smem();
     ok = wg_barrier_and(g, ok);
-    if (ok && leader) issue_layer<MODE>(p.layers[0], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+    if (ok && q == 0 && elect_one()) issue_layer<MODE>(p.layers[0], wbase, a_tmem, aux_base, d_tmem, acc_bar);
     for (int k = 0; k < K && ok; ++k) {
       for (int l = 0; l < p.n_layers; ++l) {
         const TcLayer& L = p.layers[l];
@@ -622,7 +636,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
         if (!ok) break;
-        if (leader) issue_layer<MODE>(p.layers[nl], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+        if (q == 0 && elect_one()) issue_layer<MODE>(p.layers[nl], wbase, a_tmem, aux_base, d_tmem, acc_bar);
       }
     }
     if (valid && ok) {
@@ -636,7 +650,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     ok = wg_barrier_and(g, ok);
   }
   // every MMA this warpgroup issued has completed before TMEM is released
-  if (leader) {
+  if (q == 0 && elect_one()) {  // the same lane that issued: a commit tracks its own thread's MMAs
     mma_commit(&bars->done[g]);
     wait_bounded(&bars->done[g], 0, p.err);
   }
