@@ -33,6 +33,7 @@
 // Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
 // kDevWaitTimeout and the warpgroup unwinds together.
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 
@@ -444,28 +445,49 @@ struct __align__(8) TcBarriers {
   uint32_t tmem_base;
 };
 
+// Layer sequences fixed at compile time, so that the per-layer flags are constants and the
+// layer loop unrolls (the plan still supplies offsets, strides and scales).  kShapePlan: the
+// sequence is read from the plan at run time.  Both fixed shapes have 64-wide ReLU layers,
+// one of them with the aux block and the last one fin:
+//   kShapeSix: out_prd 32->64->64->64, folded cmp_net first layer (+aux), two 64->64 layers;
+//   kShapeTwo: folded cmp_net first layer (+aux) on 16 hash features, one 64->64 layer.
+enum TcShape { kShapePlan = 0, kShapeSix = 1, kShapeTwo = 2 };
+template <int SHAPE> struct ShapeOf { static constexpr int nl = 0, aux = -1; };
+template <> struct ShapeOf<kShapeSix> { static constexpr int nl = 6, aux = 3; };
+template <> struct ShapeOf<kShapeTwo> { static constexpr int nl = 2, aux = 0; };
+
+// S K-steps of one layer, unrolled: step s reads 8 more TMEM columns of A and the next two
+// 128-byte core-matrix columns of B (+16 in the descriptor's address field, which counts
+// 16-byte units).
+template <int MODE, int S>
+__device__ __forceinline__ void issue_steps(uint32_t d_tmem, uint32_t a_tmem, uint64_t b0, uint32_t id) {
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    if constexpr (MODE == kTcFp8)
+      mma_ts_e4m3(d_tmem, a_tmem + (uint32_t)s * 8u, b0 + (uint64_t)(s * 16), id, s > 0 ? 1u : 0u);
+    else
+      mma_ts(d_tmem, a_tmem + (uint32_t)s * 8u, b0 + (uint64_t)(s * 16), id, s > 0 ? 1u : 0u);
+  }
+}
+
 // Issues layer L of warpgroup g's tile: A from TMEM (and the aux block from shared memory).
 // A K step covers 32 bytes of a row in both precisions (16 BF16 or 32 E4M3 values): 8 TMEM
 // columns of A and two 128-byte core-matrix columns of B.  The aux block stays BF16 in both;
-// its MMA accumulates into the same FP32 accumulator.
+// its MMA accumulates into the same FP32 accumulator.  The K loop is unrolled for each step
+// count the plans produce (1, 2 or 4): issuing with descriptors computed in a run-time loop
+// made every layer's round trip measurably longer.
 template <int MODE>
-__device__ __forceinline__ void issue_layer(const TcLayer& L, uint32_t wbase, uint32_t a_tmem, uint32_t aux_base,
-                                            uint32_t d_tmem, uint64_t* bar) {
+__device__ __forceinline__ void issue_layer(const TcLayer& L, bool with_aux, uint32_t wbase, uint32_t a_tmem,
+                                            uint32_t aux_base, uint32_t d_tmem, uint64_t* bar) {
   tc_fence_after();
-  if constexpr (MODE == kTcFp8) {
-    const uint32_t id = idesc_e4m3(L.n);
-    for (int s = 0; s < L.k / 32; ++s) {
-      const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
-      mma_ts_e4m3(d_tmem, a_tmem + (uint32_t)s * 8u, bd, id, s > 0 ? 1u : 0u);
-    }
-  } else {
-    const uint32_t id = idesc_bf16(L.n);
-    for (int s = 0; s < L.k / 16; ++s) {
-      const uint64_t bd = smem_desc(wbase + L.b_off + (uint32_t)s * 256u, 128u, L.b_sbo);
-      mma_ts(d_tmem, a_tmem + (uint32_t)s * 8u, bd, id, s > 0 ? 1u : 0u);
-    }
-  }
-  if (L.aux) {
+  const uint64_t b0 = smem_desc(wbase + L.b_off, 128u, L.b_sbo);
+  const uint32_t id = MODE == kTcFp8 ? idesc_e4m3(L.n) : idesc_bf16(L.n);
+  const int steps = L.k / (MODE == kTcFp8 ? 32 : 16);
+  if (steps == 4) issue_steps<MODE, 4>(d_tmem, a_tmem, b0, id);
+  else if (steps == 2) issue_steps<MODE, 2>(d_tmem, a_tmem, b0, id);
+  else if (steps == 1) issue_steps<MODE, 1>(d_tmem, a_tmem, b0, id);
+  else issue_steps<MODE, 3>(d_tmem, a_tmem, b0, id);
+  if (with_aux) {
     const uint64_t ad = smem_desc(aux_base, 128u, 256u);
     const uint64_t bd = smem_desc(wbase + L.aux_off, 128u, 256u);
     mma_ss(d_tmem, ad, bd, idesc_bf16(L.n), 1u);
@@ -473,8 +495,10 @@ __device__ __forceinline__ void issue_layer(const TcLayer& L, uint32_t wbase, ui
   mma_commit(bar);
 }
 
-template <int DMAX, int MODE>
+template <int DMAX, int MODE, int SHAPE>
 __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_constant__ TcParams p) {
+  using Sh = ShapeOf<SHAPE>;
+  const int n_layers = SHAPE ? Sh::nl : p.n_layers;
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;                                       // weight blob (+ V_last)
   uint8_t* aux = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kNWG][kAuxBytes]
@@ -555,44 +579,49 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     tc_fence_before();
     fence_proxy_async_smem();
     ok = wg_barrier_and(g, ok);
-    if (ok && q == 0 && elect_one()) issue_layer<MODE>(p.layers[0], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+    if (ok && q == 0 && elect_one()) issue_layer<MODE>(p.layers[0], SHAPE ? Sh::aux == 0 : p.layers[0].aux != 0, wbase, a_tmem, aux_base, d_tmem,
+                                                        acc_bar);
     for (int k = 0; k < K && ok; ++k) {
-      for (int l = 0; l < p.n_layers; ++l) {
+#pragma unroll(SHAPE ? Sh::nl : 1)
+      for (int l = 0; l < n_layers; ++l) {
         const TcLayer& L = p.layers[l];
+        const bool fin = SHAPE ? l == Sh::nl - 1 : L.fin != 0;
+        const bool relu = SHAPE ? true : L.relu != 0;
+        const bool wide_out = SHAPE ? true : L.n > 32;
         const bool waited = __all_sync(0xffffffffu, wait_bounded(acc_bar, ph, p.err));
         ph ^= 1u;
         if (waited) {
           tc_fence_after();
           uint32_t v[32];
-          if (!L.fin && MODE == kTcFp8) {
+          if (!fin && MODE == kTcFp8) {
             uint32_t a[8];
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
-            if (L.relu) pack32_e4m3<true>(v, L.scale, a);
+            if (relu) pack32_e4m3<true>(v, L.scale, a);
             else pack32_e4m3<false>(v, L.scale, a);
             tmem_st8(a_taddr, a);
-            if (L.n > 32) {
+            if (wide_out) {
               tmem_ld32(d_taddr + 32u, v);
               tmem_wait_ld();
-              if (L.relu) pack32_e4m3<true>(v, L.scale, a);
+              if (relu) pack32_e4m3<true>(v, L.scale, a);
               else pack32_e4m3<false>(v, L.scale, a);
               tmem_st8(a_taddr + 8u, a);
             }
             tmem_wait_st();
-          } else if (!L.fin) {
+          } else if (!fin) {
             uint32_t a[16];
             uint32_t m = 0;
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
-            if constexpr (MODE == kTcCalibrate) m = amax32(v, L.relu);
-            if (L.relu) pack32<true>(v, a);
+            if constexpr (MODE == kTcCalibrate) m = amax32(v, relu);
+            if (relu) pack32<true>(v, a);
             else pack32<false>(v, a);
             tmem_st16(a_taddr, a);
-            if (L.n > 32) {
+            if (wide_out) {
               tmem_ld32(d_taddr + 32u, v);
               tmem_wait_ld();
-              if constexpr (MODE == kTcCalibrate) m = max(m, amax32(v, L.relu));
-              if (L.relu) pack32<true>(v, a);
+              if constexpr (MODE == kTcCalibrate) m = max(m, amax32(v, relu));
+              if (relu) pack32<true>(v, a);
               else pack32<false>(v, a);
               tmem_st16(a_taddr + 16u, a);
             }
@@ -608,7 +637,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             final_dot32x2(v, sV, 0, q0, q1, q2);
             tmem_ld32(d_taddr + 32u, v);
             tmem_wait_ld();
-            if constexpr (MODE == kTcCalibrate) record_amax(p.amax + p.n_layers, max(m, amax32(v, true)));
+            if constexpr (MODE == kTcCalibrate) record_amax(p.amax + n_layers, max(m, amax32(v, true)));
             final_dot32x2(v, sV, 32, q0, q1, q2);
             t0 = sum2(q0); t1 = sum2(q1); t2 = sum2(q2);
             const float* Lk = J.strength + (size_t)k * 3;
@@ -631,12 +660,14 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
           }
         }
         ok = ok && waited;
-        if (l + 1 == p.n_layers && k + 1 == K) break;  // the tile's last layer: no hand-off
-        const int nl = (l + 1 == p.n_layers) ? 0 : l + 1;
+        if (l + 1 == n_layers && k + 1 == K) break;  // the tile's last layer: no hand-off
+        const int nl = (l + 1 == n_layers) ? 0 : l + 1;
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
         if (!ok) break;
-        if (q == 0 && elect_one()) issue_layer<MODE>(p.layers[nl], wbase, a_tmem, aux_base, d_tmem, acc_bar);
+        if (q == 0 && elect_one())
+          issue_layer<MODE>(p.layers[nl], SHAPE ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
+                            d_tmem, acc_bar);
       }
     }
     if (valid && ok) {
@@ -928,6 +959,21 @@ TcPlan pack_tc_weights_fp8(const NetDims& d, const float* op, const float* cn, c
   return P;
 }
 
+// The compile-time layer sequence that matches plan P (kShapePlan if none does).
+int shape_of(const TcPlan& P, const NetDims& d) {
+  auto fixed = [&](int nl, int aux, int enc) {
+    if (P.n_layers != nl || d.enc_dims() != enc) return false;
+    for (int l = 0; l < nl; ++l) {
+      const TcLayer& L = P.layers[l];
+      if (L.n != 64 || !L.relu || (L.aux != 0) != (l == aux) || (L.fin != 0) != (l == nl - 1)) return false;
+    }
+    return true;
+  };
+  if (fixed(ShapeOf<kShapeSix>::nl, ShapeOf<kShapeSix>::aux, 32)) return kShapeSix;
+  if (fixed(ShapeOf<kShapeTwo>::nl, ShapeOf<kShapeTwo>::aux, 16)) return kShapeTwo;
+  return kShapePlan;
+}
+
 size_t enc_smem_bytes(const NetDims& d) { return (size_t)kNWG * (d.enc_dims() <= 16 ? 8 : 16) * kTile * 4; }
 
 size_t relight_tc_smem_bytes(const NetDims& d) {
@@ -987,11 +1033,18 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
     NWPRT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kThreads, smem, st>>>(p);
   };
-  const bool wide = d.enc_dims() > 16;
+  const int shape = shape_of(P, d);
+  auto pick = [&](auto mode_tag) {
+    constexpr int M = decltype(mode_tag)::value;
+    if (shape == kShapeSix) go(relight_tc_kernel<32, M, kShapeSix>);
+    else if (shape == kShapeTwo) go(relight_tc_kernel<16, M, kShapeTwo>);
+    else if (d.enc_dims() > 16) go(relight_tc_kernel<32, M, kShapePlan>);
+    else go(relight_tc_kernel<16, M, kShapePlan>);
+  };
   switch (mode) {
-    case kTcBf16: wide ? go(relight_tc_kernel<32, kTcBf16>) : go(relight_tc_kernel<16, kTcBf16>); break;
-    case kTcCalibrate: wide ? go(relight_tc_kernel<32, kTcCalibrate>) : go(relight_tc_kernel<16, kTcCalibrate>); break;
-    case kTcFp8: wide ? go(relight_tc_kernel<32, kTcFp8>) : go(relight_tc_kernel<16, kTcFp8>); break;
+    case kTcBf16: pick(std::integral_constant<int, kTcBf16>{}); break;
+    case kTcCalibrate: pick(std::integral_constant<int, kTcCalibrate>{}); break;
+    case kTcFp8: pick(std::integral_constant<int, kTcFp8>{}); break;
     default: fail(NWPRT_INVALID_ARG, "unknown tensor-core mode");
   }
   NWPRT_CUDA(cudaGetLastError());
