@@ -90,6 +90,7 @@ struct nwprt_ctx {
   std::vector<float> h_op, h_cn;
   uint8_t* d_tc_w8 = nullptr;
   TcPlan fp8_plan{};
+  TcPlan bf16_plan{};
   bool fp8_ready = false;
   std::vector<float> fp8_amax;
   std::vector<EnvEntry> envs;
@@ -345,7 +346,7 @@ nwprt_status nwprt_load_weights(nwprt_ctx* ctx, const nwprt_weights* w) {
     ctx->h_cn.assign(w->cmp_net, w->cmp_net + w->n_cmp_net);
     if (ctx->tc_supported) {
       std::vector<uint16_t> tw;
-      pack_tc_weights(d, w->out_prd, w->cmp_net, &tw);
+      ctx->bf16_plan = pack_tc_weights(d, w->out_prd, w->cmp_net, &tw);
       ctx->d_tc_w = dev_alloc<uint16_t>(tw.size());
       NWPRT_CUDA(cudaMemcpy(ctx->d_tc_w, tw.data(), tw.size() * 2, cudaMemcpyHostToDevice));
     }
@@ -560,7 +561,7 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w8, &ctx->fp8_plan, mode, jobs.data(),
                       (int)jobs.size(), o.kahan, o.clamp_terms, nullptr, ctx->d_err, st);
   else
-    launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, nullptr, mode, jobs.data(), (int)jobs.size(),
+    launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, &ctx->bf16_plan, mode, jobs.data(), (int)jobs.size(),
                       o.kahan, o.clamp_terms, amax, ctx->d_err, st);
 }
 

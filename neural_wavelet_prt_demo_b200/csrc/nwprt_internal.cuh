@@ -174,6 +174,7 @@ struct TcPlan {
   uint32_t vlast_off = 0;   // byte offset of V_last (FP32 [3][64]) in the blob
   uint32_t blob_bytes = 0;
   float cp_scale = 1.f;     // FP8: scale of the first layer's operand hash(p) * E_k
+  float vlast[3][64] = {};  // V_last as stored in the blob (filled when the weights are given)
 };
 enum TcMode { kTcBf16 = 0, kTcCalibrate = 1, kTcFp8 = 2 };
 bool relight_tc_supported(const NetDims& d, std::string* why);
@@ -181,7 +182,8 @@ bool relight_tc_supported(const NetDims& d, std::string* why);
 void launch_wait_selftest(int timeout_ms, uint32_t* err, cudaStream_t st);
 bool relight_tc_fp8_supported(const NetDims& d, std::string* why);
 size_t tc_weight_bytes(const NetDims& d);
-void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);
+// BF16 weight blob; returns its plan (with V_last), which every BF16 launch needs.
+TcPlan pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);
 // FP8 weight blob from calibrated activation maxima amax[0..n_layers) (the input of every
 // tensor-core layer); returns the plan whose scales the kernel applies.
 TcPlan pack_tc_weights_fp8(const NetDims& d, const float* op, const float* cn, const float* amax,
@@ -201,7 +203,7 @@ struct TcJob {
   long long tile_begin;   // first 128-pixel tile of this job in the launch (set by the launcher)
   int64_t px_begin;       // start of the pixel range
 };
-// mode kTcBf16 / kTcCalibrate use the BF16 blob (plan == nullptr: derived from d);
+// mode kTcBf16 / kTcCalibrate use the BF16 blob and its plan (from pack_tc_weights);
 // kTcCalibrate also records per-layer activation maxima into amax (uint bits of floats);
 // kTcFp8 uses the FP8 blob and its plan.
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,

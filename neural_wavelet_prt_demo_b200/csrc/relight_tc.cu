@@ -74,7 +74,11 @@ struct TcParams {
   float cp_scale;   // FP8: scale of the first layer's operand
   uint32_t* amax;   // calibration: per-layer activation maxima (float bits)
   uint32_t* err;
+  // V_last, the FP32 3 x 64 output layer.  From the parameter space every output-dot FMA
+  // takes its weight pair as an operand, without a shared-memory load.
+  float vlast[3][64];
 };
+static_assert(sizeof(TcParams) <= 32764, "kernel parameters are limited to 32,764 bytes");
 
 // ------------------------------------------------------------------ PTX wrappers
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -325,19 +329,17 @@ __device__ __forceinline__ float sum2(unsigned long long x) {
   return __fadd_rn(lo, hi);
 }
 // T += V_last[:, j0:j0+32] relu(h[j0:j0+32]) in FP32 with packed FMAs: q_c holds the
-// partial sums of channel c over even and odd j, added once at the end (sum2).
-__device__ __forceinline__ void final_dot32x2(const uint32_t (&v)[32], const float* __restrict__ sV, int j0,
+// partial sums of channel c over even and odd j, added once at the end (sum2).  V is the
+// kernel-parameter copy of V_last.
+__device__ __forceinline__ void final_dot32x2(const uint32_t (&v)[32], const float (&V)[3][64], int j0,
                                               unsigned long long& q0, unsigned long long& q1, unsigned long long& q2) {
 #pragma unroll
-  for (int j4 = 0; j4 < 8; ++j4) {
-    const float4 a = *reinterpret_cast<const float4*>(sV + 0 * 64 + j0 + 4 * j4);
-    const float4 b = *reinterpret_cast<const float4*>(sV + 1 * 64 + j0 + 4 * j4);
-    const float4 c = *reinterpret_cast<const float4*>(sV + 2 * 64 + j0 + 4 * j4);
-    const unsigned long long h01 = pk2(fmaxf(__uint_as_float(v[4 * j4 + 0]), 0.f), fmaxf(__uint_as_float(v[4 * j4 + 1]), 0.f));
-    const unsigned long long h23 = pk2(fmaxf(__uint_as_float(v[4 * j4 + 2]), 0.f), fmaxf(__uint_as_float(v[4 * j4 + 3]), 0.f));
-    fma2(q0, pk2(a.x, a.y), h01); fma2(q0, pk2(a.z, a.w), h23);
-    fma2(q1, pk2(b.x, b.y), h01); fma2(q1, pk2(b.z, b.w), h23);
-    fma2(q2, pk2(c.x, c.y), h01); fma2(q2, pk2(c.z, c.w), h23);
+  for (int j2 = 0; j2 < 16; ++j2) {
+    const int j = j0 + 2 * j2;
+    const unsigned long long h = pk2(fmaxf(__uint_as_float(v[2 * j2]), 0.f), fmaxf(__uint_as_float(v[2 * j2 + 1]), 0.f));
+    fma2(q0, pk2(V[0][j], V[0][j + 1]), h);
+    fma2(q1, pk2(V[1][j], V[1][j + 1]), h);
+    fma2(q2, pk2(V[2][j], V[2][j + 1]), h);
   }
 }
 
@@ -533,7 +535,6 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   tc_fence_after();
   const uint32_t tmem = bars->tmem_base;
   const uint32_t wbase = smem_u32(wsm);
-  const float* sV = reinterpret_cast<const float*>(wsm + p.vlast_off);
   const long long stride = (long long)gridDim.x * kNWG;
   const uint32_t col0 = tmem + (uint32_t)(g * kTileCols);
   const uint32_t a_tmem = col0 + kAcol;                                 // MMA operand address (lane 0)
@@ -634,11 +635,11 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             tmem_wait_ld();
             if constexpr (MODE == kTcCalibrate) m = amax32(v, true);
             unsigned long long q0 = 0ull, q1 = 0ull, q2 = 0ull;
-            final_dot32x2(v, sV, 0, q0, q1, q2);
+            final_dot32x2(v, p.vlast, 0, q0, q1, q2);
             tmem_ld32(d_taddr + 32u, v);
             tmem_wait_ld();
             if constexpr (MODE == kTcCalibrate) record_amax(p.amax + n_layers, max(m, amax32(v, true)));
-            final_dot32x2(v, sV, 32, q0, q1, q2);
+            final_dot32x2(v, p.vlast, 32, q0, q1, q2);
             t0 = sum2(q0); t1 = sum2(q1); t2 = sum2(q2);
             const float* Lk = J.strength + (size_t)k * 3;
             float u0 = __fmul_rn(__ldg(Lk + 0), t0);
@@ -853,6 +854,7 @@ TcPlan make_plan(const NetDims& d, const float* op, const float* cn, int eb, con
       for (int j = 0; j < 64; ++j) {
         const float v = j < n_in ? w[(size_t)c * n_in + j] * inv : 0.f;
         std::memcpy(blob->data() + off + (c * 64 + j) * 4, &v, 4);
+        P.vlast[c][j] = v;
       }
   }
   off += vbytes;
@@ -916,11 +918,12 @@ int tc_layer_count(const NetDims& d) { return d.op_nl + d.cn_nl - 2; }
 
 size_t tc_weight_bytes(const NetDims& d) { return plan_bf16(d, nullptr, nullptr, nullptr).blob_bytes; }
 
-void pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out) {
+TcPlan pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out) {
   std::vector<uint8_t> b;
-  plan_bf16(d, op, cn, &b);
+  const TcPlan P = plan_bf16(d, op, cn, &b);
   out->assign(b.size() / 2, 0);
   std::memcpy(out->data(), b.data(), b.size());
+  return P;
 }
 
 // Per-layer FP8 scales.  h[l] = kTarget / amax[l] maps layer l's input activations to
@@ -988,6 +991,7 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   if (!plan_supported(d, &why)) fail(NWPRT_UNSUPPORTED, why);
   if (n_jobs <= 0) return;
   if (mode == kTcFp8 && !plan) fail(NWPRT_NOT_READY, "FP8 relight without a calibrated plan");
+  if (!plan) fail(NWPRT_NOT_READY, "tensor-core relight without packed weights");
   if (mode == kTcCalibrate && !amax) fail(NWPRT_INVALID_ARG, "calibration needs an amax buffer");
   if (n_jobs > kInlineJobs) {
     for (int j0 = 0; j0 < n_jobs; j0 += kInlineJobs)
@@ -995,13 +999,14 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
                         clamp, amax, err, st);
     return;
   }
-  const TcPlan P = mode == kTcFp8 ? *plan : plan_bf16(d, nullptr, nullptr, nullptr);
+  const TcPlan& P = *plan;
   TcParams p{};
   p.hl = hl;
   p.hash = hash;
   p.wblob = reinterpret_cast<const uint4*>(blob_dev);
   p.wblob_bytes = P.blob_bytes;
   p.vlast_off = P.vlast_off;
+  std::memcpy(p.vlast, P.vlast, sizeof(p.vlast));
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
   p.n_layers = P.n_layers;
   p.enc_dims = d.enc_dims();
