@@ -50,9 +50,14 @@ struct EnvEntry {
   int cap = 0;                // wavelets the buffers below can hold (kept across reuse)
   int32_t* idx = nullptr;
   float* strength = nullptr;
-  float* emb_k = nullptr;     // [K][D], valid when emb_ready
+  float* emb_k = nullptr;     // [K][D], valid when emb_ready; then [cap][D/2] BF16 pairs
   bool emb_ready = false;
 };
+
+// The BF16 pairs of an env's embedding rows, stored after the FP32 rows.
+const uint32_t* emb_pairs(const EnvEntry& e, int D) {
+  return reinterpret_cast<const uint32_t*>(e.emb_k + (size_t)e.cap * D);
+}
 
 void free_env_buffers(EnvEntry& e) {
   dev_free(e.idx);
@@ -176,7 +181,8 @@ void ensure_emb(nwprt_ctx* ctx, EnvEntry& e, cudaStream_t st) {
   if (e.emb_ready) return;
   need(ctx->weights_loaded, NWPRT_NOT_READY, "weights are not loaded");
   const int D = ctx->dims.enc_dims();
-  launch_gather_embedding(ctx->d_emb, D, ctx->dims.n_coeffs(), e.idx, e.K, e.emb_k, ctx->d_err, st);
+  launch_gather_embedding(ctx->d_emb, D, ctx->dims.n_coeffs(), e.idx, e.K, e.emb_k,
+                          const_cast<uint32_t*>(emb_pairs(e, D)), ctx->d_err, st);
   e.emb_ready = true;
 }
 
@@ -203,7 +209,7 @@ int new_env(nwprt_ctx* ctx, int K, int D) {
     EnvEntry& e = ctx->envs[id];
     e.idx = dev_alloc<int32_t>(K);
     e.strength = dev_alloc<float>((size_t)K * 3);
-    e.emb_k = dev_alloc<float>((size_t)K * D);
+    e.emb_k = dev_alloc<float>((size_t)K * D + (size_t)K * (D / 2));
     e.cap = K;
   }
   EnvEntry& e = ctx->envs[id];
@@ -554,7 +560,7 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
     ensure_emb(ctx, e, st);
     if (r.px_end == r.px_begin) continue;
     jobs.push_back(TcJob{f.packed, f.flag, f.direct, e.emb_k, e.strength, e.K, r.px_end, r.indirect, r.with_direct,
-                         0, r.px_begin});
+                         0, r.px_begin, emb_pairs(e, ctx->dims.enc_dims())});
   }
   if (jobs.empty()) return;
   if (mode == kTcFp8)

@@ -113,8 +113,10 @@ void launch_env_rotate(const float* src, int S, const float* R_host, float* dst,
 
 // relight_common.cu
 void launch_pack_gbuffer(const nwprt_gbuffer& g, float* packed, cudaStream_t st);
+// out_kd: [K][D] FP32 rows; out_h (may be null): the same rows as BF16 pairs, [K][D/2]
+// 32-bit words with feature 2i in the low half (D even).
 void launch_gather_embedding(const float* emb, int D, int n_coeffs, const int32_t* idx, int K,
-                             float* out_kd, uint32_t* err, cudaStream_t st);
+                             float* out_kd, uint32_t* out_h, uint32_t* err, cudaStream_t st);
 
 // One relight job: a prepared frame and an env wavelet table.
 struct RelightJob {
@@ -202,6 +204,7 @@ struct TcJob {
   float* with_direct;
   long long tile_begin;   // first 128-pixel tile of this job in the launch (set by the launcher)
   int64_t px_begin;       // start of the pixel range
+  const uint32_t* emb_h;  // [K][D/2] the same rows as BF16 pairs (the BF16 form's operand)
 };
 // mode kTcBf16 / kTcCalibrate use the BF16 blob and its plan (from pack_tc_weights);
 // kTcCalibrate also records per-layer activation maxima into amax (uint bits of floats);

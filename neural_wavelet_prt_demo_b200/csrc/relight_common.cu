@@ -31,20 +31,29 @@ __global__ void pack_gbuffer_kernel(int64_t n, const float4* __restrict__ pos,
   out[p * 4 + 3] = make_float4(2.f * d.z - 1.f, 2.f * e.x - 1.f, 2.f * e.y - 1.f, 2.f * e.z - 1.f);
 }
 
+// One thread per feature pair (k, 2i..2i+1): both FP32 values, and (out_h) their BF16 pair.
 __global__ void gather_embedding_kernel(const float* __restrict__ emb, int D, int n_coeffs,
                                         const int32_t* __restrict__ idx, int K,
-                                        float* __restrict__ out, uint32_t* err) {
+                                        float* __restrict__ out, uint32_t* __restrict__ out_h, uint32_t* err) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)K * D) return;
-  const int k = (int)(t / D), d = (int)(t - (int64_t)k * D);
+  const int H = D / 2;
+  if (t >= (int64_t)K * H) return;
+  const int k = (int)(t / H), d = 2 * (int)(t - (int64_t)k * H);
   const int32_t j = idx[k];
-  float v = 0.f;
+  float v0 = 0.f, v1 = 0.f;
   if (j >= 0 && j < n_coeffs) {
-    v = emb[(int64_t)d * n_coeffs + j];
+    v0 = emb[(int64_t)d * n_coeffs + j];
+    v1 = emb[(int64_t)(d + 1) * n_coeffs + j];
   } else if (err) {
     atomicCAS(err, 0u, (uint32_t)kDevBadIndex);
   }
-  out[t] = v;
+  out[(int64_t)k * D + d] = v0;
+  out[(int64_t)k * D + d + 1] = v1;
+  if (out_h) {
+    uint32_t h;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(v1), "f"(v0));
+    out_h[t] = h;
+  }
 }
 
 }  // namespace
@@ -62,11 +71,12 @@ void launch_pack_gbuffer(const nwprt_gbuffer& g, float* packed, cudaStream_t st)
 }
 
 void launch_gather_embedding(const float* emb, int D, int n_coeffs, const int32_t* idx, int K,
-                             float* out_kd, uint32_t* err, cudaStream_t st) {
-  const int64_t n = (int64_t)K * D;
+                             float* out_kd, uint32_t* out_h, uint32_t* err, cudaStream_t st) {
+  if (D % 2) fail(NWPRT_UNSUPPORTED, "embedding gather needs an even feature count");
+  const int64_t n = (int64_t)K * (D / 2);
   if (n == 0) return;
   gather_embedding_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(emb, D, n_coeffs, idx, K,
-                                                                        out_kd, err);
+                                                                        out_kd, out_h, err);
   NWPRT_CUDA(cudaGetLastError());
 }
 

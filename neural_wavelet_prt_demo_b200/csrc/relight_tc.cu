@@ -386,14 +386,31 @@ __device__ __forceinline__ void hash_encode_bf16(const HashLevels& hl, const flo
   }
 }
 
-// First-layer operand of wavelet k, hash(p) * E_k -> TMEM A columns: rounded once to BF16,
-// or (FP8) scaled by cp_scale and rounded to E4M3, zero-padded to K = 32.  Calibration
-// records max |hash(p) * E_k| in amax[0].
+// First-layer operand of wavelet k, hash(p) * E_k -> TMEM A columns.  BF16: one packed
+// bf16x2 multiply per feature pair of the BF16 hash features and the BF16 embedding row eh
+// (the exact product, rounded once).  Calibration: the same product from the FP32 row ek,
+// recording max |hash(p) * E_k| in amax[0].  FP8: from the FP32 row, scaled by cp_scale and
+// rounded to E4M3, zero-padded to K = 32.
 template <int DMAX, int MODE>
-__device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __restrict__ ek, uint32_t a_taddr,
-                                         float cp_scale, uint32_t* amax) {
+__device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __restrict__ ek,
+                                         const uint32_t* __restrict__ eh, uint32_t a_taddr, float cp_scale,
+                                         uint32_t* amax) {
   constexpr int NW = MODE == kTcFp8 ? 8 : DMAX / 2;
   uint32_t cp[NW];
+  if constexpr (MODE == kTcBf16) {
+#pragma unroll
+    for (int c = 0; c < DMAX / 8; ++c) {
+      const uint4 e = __ldg(reinterpret_cast<const uint4*>(eh) + c);
+      const uint32_t ev[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(cp[c * 4 + i]) : "r"(enc_s[(c * 4 + i) * kTile]), "r"(ev[i]));
+      }
+    }
+    if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
+    else tmem_st8(a_taddr, cp);
+    return;
+  }
   float m = 0.f;
 #pragma unroll
   for (int c = 0; c < DMAX / 8; ++c) {
@@ -573,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
       st_shared_v4(aux_row, 0, 0, 0, 0);
       st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
     }
-    store_cp<DMAX, MODE>(enc_s, J.emb_k, a_taddr, p.cp_scale, p.amax);
+    store_cp<DMAX, MODE>(enc_s, J.emb_k, J.emb_h, a_taddr, p.cp_scale, p.amax);
     tmem_wait_st();
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     // hand the first layer to the tensor core
@@ -655,7 +672,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
               s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
             }
             if (k + 1 < K) {
-              store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims, a_taddr, p.cp_scale, p.amax);
+              store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims,
+                                   J.emb_h + (size_t)(k + 1) * (p.enc_dims / 2), a_taddr, p.cp_scale, p.amax);
               tmem_wait_st();
             }
           }
