@@ -365,10 +365,10 @@ def run_ours(args):
     if precision == "bf16":
         peak = peaks.get("bf16_tflops_sustained") or peaks["bf16_tflops"]
         # DRAM bytes per launch from one ncu capture of this kernel on the same 1920x1080 frame
-        # (dram__bytes_read.sum + dram__bytes_write.sum = 251.1 + 65.1 MB at K=8); the kernel
+        # (dram__bytes_read.sum + dram__bytes_write.sum = 337.0 + 63.3 MB at K=8); the kernel
         # reads each pixel's inputs and writes its outputs once, so the traffic does not depend
         # on K and scales with the pixel count.
-        traffic = 316.2e6 * N / (1920 * 1080)
+        traffic = 400.3e6 * N / (1920 * 1080)
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "traffic_source": "ncu dram bytes of relight_tc_kernel, 1920x1080 K=8 capture, K-independent",
