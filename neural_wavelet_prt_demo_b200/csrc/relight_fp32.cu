@@ -231,6 +231,143 @@ __global__ void __launch_bounds__(NT, 1) relight_fp32_kernel(Fp32Params p) {
   }
 }
 
+// ---- any other supported network: the same arithmetic with the layer sequence read at run
+// time.  Every dot product still accumulates fmaf(W[j][i], x_i, .) from 0 in ascending i, so
+// results are the same bits as the oracle's.  Output widths up to kGenMaxOut.
+constexpr int kGenMaxOut = 64;
+constexpr int kGenMaxLayers = 2 * kMaxLayers;
+struct GenLayer {
+  int in, out, relu, mode;  // mode as in dense(): 0 plain, 1 CP product, 2 [out_prd || aux]
+  int w_off;                // float offset of the [in][round4(out)] block
+};
+struct GenNet {
+  GenLayer l[kGenMaxLayers];
+  int n = 0;
+  int enc = 0, aux = 0, rows = 0, opo = 0, d = 0, auxw = 0;
+};
+
+template <int NT>
+__device__ __forceinline__ void dense_rt(const GenLayer& L, const GenNet& g, const float* __restrict__ Wt,
+                                         float* act, const float* __restrict__ e, float* outv) {
+  float acc[kGenMaxOut];
+#pragma unroll
+  for (int j = 0; j < kGenMaxOut; ++j) acc[j] = 0.f;
+  const int o4 = (L.out + 3) / 4;
+  for (int i = 0; i < L.in; ++i) {
+    float xi;
+    if (L.mode == 0) xi = act[i * NT];
+    else if (L.mode == 1) xi = __fmul_rn(act[(g.enc + i) * NT], e[i]);
+    else xi = (i < g.opo) ? act[i * NT] : act[(g.aux + i - g.opo) * NT];
+    const float4* w4 = reinterpret_cast<const float4*>(Wt + (size_t)i * o4 * 4);
+#pragma unroll
+    for (int j = 0; j < kGenMaxOut / 4; ++j) {
+      if (j < o4) {
+        const float4 w = w4[j];
+        acc[4 * j + 0] = fmaf(w.x, xi, acc[4 * j + 0]);
+        acc[4 * j + 1] = fmaf(w.y, xi, acc[4 * j + 1]);
+        acc[4 * j + 2] = fmaf(w.z, xi, acc[4 * j + 2]);
+        acc[4 * j + 3] = fmaf(w.w, xi, acc[4 * j + 3]);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kGenMaxOut; ++j) {
+    if (j < L.out) {
+      const float v = L.relu ? fmaxf(acc[j], 0.f) : acc[j];
+      if (outv) outv[j] = v;
+      else act[j * NT] = v;
+    }
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) relight_fp32_generic_kernel(Fp32Params p, const __grid_constant__ GenNet g) {
+  extern __shared__ __align__(16) float sm[];
+  float* sW = sm;
+  float* sE = sW + p.w_floats;
+  float* sL = sE + kMaxKChunk * g.d;
+  float* sAct = sL + kMaxKChunk * 4;
+  const int tid = threadIdx.x;
+  for (int i = tid * 4; i < p.w_floats; i += NT * 4)
+    *reinterpret_cast<float4*>(sW + i) = __ldg(reinterpret_cast<const float4*>(p.w + i));
+  const int64_t px = p.px_begin + (int64_t)blockIdx.x * NT + tid;
+  const bool valid = px < p.n_px;
+  const bool active = valid && p.flag[px] != 0;
+  float* act = sAct + tid;
+  if (valid) {
+    const float4* row = reinterpret_cast<const float4*>(p.packed) + px * 4;
+    const float4 r0 = row[0], r1 = row[1], r2 = row[2], r3 = row[3];
+    if (active) hash_encode(p.hl, p.hash, r0.x, r0.y, r0.z, act, NT, g.enc);
+    const float aux13[13] = {r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+    for (int i = 0; i < g.auxw; ++i) act[(g.aux + i) * NT] = i < 13 ? aux13[i] : 1.0f;
+  }
+  float s[3] = {0.f, 0.f, 0.f}, comp[3] = {0.f, 0.f, 0.f};
+  for (int k0 = 0; k0 < p.K; k0 += kMaxKChunk) {
+    const int kc = min(kMaxKChunk, p.K - k0);
+    __syncthreads();
+    for (int i = tid; i < kc * g.d; i += NT) sE[i] = p.emb_k[(size_t)k0 * g.d + i];
+    for (int i = tid; i < kc * 3; i += NT) sL[(i / 3) * 4 + i % 3] = p.strength[(size_t)k0 * 3 + i];
+    __syncthreads();
+    if (!active) continue;
+    for (int kk = 0; kk < kc; ++kk) {
+      float T[3];
+      for (int li = 0; li < g.n; ++li)
+        dense_rt<NT>(g.l[li], g, sW + g.l[li].w_off, act, sE + kk * g.d, li + 1 == g.n ? T : nullptr);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float term = __fmul_rn(sL[kk * 4 + c], T[c]);
+        if (p.clamp) term = fmaxf(term, 0.0f);
+        if (p.kahan) {
+          const float y = __fsub_rn(term, comp[c]);
+          const float t = __fadd_rn(s[c], y);
+          comp[c] = __fsub_rn(__fsub_rn(t, s[c]), y);
+          s[c] = t;
+        } else {
+          s[c] = __fadd_rn(s[c], term);
+        }
+      }
+    }
+  }
+  if (valid) {
+    const float4 dl = reinterpret_cast<const float4*>(p.direct)[px];
+    reinterpret_cast<float4*>(p.indirect)[px] = make_float4(s[0], s[1], s[2], 1.f);
+    reinterpret_cast<float4*>(p.with_direct)[px] =
+        make_float4(__fadd_rn(s[0], dl.x), __fadd_rn(s[1], dl.y), __fadd_rn(s[2], dl.z), 1.f);
+  }
+}
+
+// The run-time layer sequence of d: out_prd's layers (the first takes the CP product), then
+// cmp_net's (the first takes [out_prd || aux]); the last layer writes T.
+bool gen_net(const NetDims& d, GenNet* g, std::string* why) {
+  auto no = [&](const char* m) { if (why) *why = m; return false; };
+  if (d.op_nl + d.cn_nl > kGenMaxLayers) return no("fp32 relight: too many layers");
+  int off = 0, widest = d.op_out;
+  for (int i = 0; i < d.op_nl; ++i) {
+    if (d.op_outs[i] > kGenMaxOut) return no("fp32 relight: layer widths above 64 are not supported");
+    g->l[g->n++] = GenLayer{d.op_in[i], d.op_outs[i], i + 1 < d.op_nl ? 1 : 0, i == 0 ? 1 : 0, off};
+    off += d.op_in[i] * r4(d.op_outs[i]);
+    widest = d.op_outs[i] > widest ? d.op_outs[i] : widest;
+  }
+  for (int i = 0; i < d.cn_nl; ++i) {
+    if (d.cn_outs[i] > kGenMaxOut) return no("fp32 relight: layer widths above 64 are not supported");
+    g->l[g->n++] = GenLayer{d.cn_in[i], d.cn_outs[i], i + 1 < d.cn_nl ? 1 : 0, i == 0 ? 2 : 0, off};
+    off += d.cn_in[i] * r4(d.cn_outs[i]);
+    if (i + 1 < d.cn_nl) widest = d.cn_outs[i] > widest ? d.cn_outs[i] : widest;
+  }
+  if (d.cn_outs[d.cn_nl - 1] != 3) return no("fp32 relight: cmp_net must end in 3 outputs");
+  g->d = d.enc_dims();
+  g->opo = d.op_out;
+  g->auxw = d.aux_width;
+  g->enc = widest;
+  g->aux = widest + g->d;
+  g->rows = g->aux + g->auxw;
+  return true;
+}
+
+size_t gen_smem_bytes(const GenNet& g, int w_floats, int nt) {
+  return sizeof(float) * ((size_t)w_floats + kMaxKChunk * g.d + kMaxKChunk * 4 + (size_t)g.rows * nt);
+}
+
 template <int D, int OPH, int OPO, int CNH, int W, int AUXW>
 bool try_launch(const NetDims& d, const Fp32Params& p, cudaStream_t st) {
   if (d.enc_dims() != D || d.op_hidden != OPH || d.op_out != OPO || d.cn_hidden != CNH ||
@@ -279,15 +416,21 @@ void pack_fp32_weights(const NetDims& d, const float* op, const float* cn, std::
   pack(d.cn_nl, d.cn_in, d.cn_outs, cn, cn_t);
 }
 
+// The two standard shapes run compile-time kernels; every other network whose layers are at
+// most 64 wide (and whose weights fit in shared memory) runs the generic kernel.
 bool relight_fp32_supported(const NetDims& d, std::string* why) {
-  const bool small = d.enc_dims() == 16 && d.op_hidden == 0 && d.op_out == 26 && d.cn_hidden == 2 &&
-                     d.cn_neurons == 64 && d.aux_width == 16;
-  const bool large = d.enc_dims() == 32 && d.op_hidden == 3 && d.op_neurons == 64 && d.op_out == 64 &&
-                     d.cn_hidden == 3 && d.cn_neurons == 64 && d.aux_width == 16;
-  if (!small && !large && why)
-    *why = "fp32 relight is instantiated for two network shapes: 16->26 | 42->64->64->3 and "
-           "32->64x3->64 | 80->64x3->3";
-  return small || large;
+  GenNet g;
+  if (!gen_net(d, &g, why)) return false;
+  int dev = 0, max_smem = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    max_smem = 227 * 1024;
+  const int w_floats = (int)(d.n_op_params() + d.n_cn_params());  // lower bound of the padded size
+  if (gen_smem_bytes(g, w_floats, 128) > (size_t)max_smem) {
+    if (why) *why = "fp32 relight: network too large for shared memory";
+    return false;
+  }
+  return true;
 }
 
 void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWeights& w,
@@ -312,9 +455,21 @@ void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWei
   p.kahan = kahan;
   if (try_launch<16, 0, 26, 2, 64, 16>(d, p, st)) return;
   if (try_launch<32, 3, 64, 3, 64, 16>(d, p, st)) return;
+  GenNet g;
   std::string why;
-  relight_fp32_supported(d, &why);
-  fail(NWPRT_UNSUPPORTED, why);
+  if (!gen_net(d, &g, &why)) fail(NWPRT_UNSUPPORTED, why);
+  const GenLayer& last = g.l[g.n - 1];
+  if (last.w_off + last.in * r4(last.out) != p.w_floats) fail(NWPRT_INVALID_ARG, "fp32 weight layout mismatch");
+  int dev = 0, max_smem = 0;
+  NWPRT_CUDA(cudaGetDevice(&dev));
+  NWPRT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t smem = gen_smem_bytes(g, p.w_floats, 128);
+  if (smem > (size_t)max_smem) fail(NWPRT_UNSUPPORTED, "fp32 relight: network too large for shared memory");
+  auto k = relight_fp32_generic_kernel<128>;
+  NWPRT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t n = p.n_px - p.px_begin;
+  k<<<(unsigned)((n + 127) / 128), 128, smem, st>>>(p, g);
+  NWPRT_CUDA(cudaGetLastError());
 }
 
 }  // namespace nwprt
