@@ -53,6 +53,10 @@ def parse_args():
     ap.add_argument("--sweep-px", type=int, default=4096, help="pixels checked against the FP64 oracle per K")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=120.0)
+    ap.add_argument("--serve-quantum-ms", type=float, default=12.0,
+                    help="serve: kernel time per scheduling quantum")
+    ap.add_argument("--serve-nets", choices=["both", "large", "small"], default="both",
+                    help="serve: which network(s) to run (config 2, config 0, or both)")
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
                     help="requests of the stream also served by the plain FP32 serial baseline")
     ap.add_argument("--fp8-steps", type=int, default=5, help="timed steps of the FP8 form (0: skip)")
@@ -707,17 +711,23 @@ def run_serve(args, rank, world, local, dev):
     from neural_wavelet_prt_demo_b200 import netconfig, serve
     out = {}
     sampler = ClockSampler(local)
-    for name, cfg, S in (("served_bf16", netconfig.CONFIG_LARGE, 64),
-                         ("served_bf16_small_net", netconfig.CONFIG_SMALL, 32)):
+    nets = [("served_bf16", netconfig.CONFIG_LARGE, 64), ("served_bf16_small_net", netconfig.CONFIG_SMALL, 32)]
+    if args.serve_nets == "large":
+        nets = nets[:1]
+    elif args.serve_nets == "small":
+        nets = nets[1:]
+    clocks = None
+    for name, cfg, S in nets:
         e, frames, base = _serve_rig(cfg, S, dev)
         rate = _measure_rate(e, frames, base, "bf16")
         reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=rank, face_size=S)
-        srv = serve.RelightServer(e, frames, base, precision="bf16", budget_bytes=150 << 30, quantum_ms=12.0,
-                                  est_evals_per_s=rate)
-        if name == "served_bf16":
+        srv = serve.RelightServer(e, frames, base, precision="bf16", budget_bytes=150 << 30,
+                                  quantum_ms=args.serve_quantum_ms, est_evals_per_s=rate)
+        first = clocks is None
+        if first:
             sampler.start()
         st = srv.run(reqs)
-        if name == "served_bf16":
+        if first:
             clocks = sampler.stop()
         st.update({"quanta": srv.quanta, "max_concurrent": srv.max_active, "kernel_evals_per_s_1080p": rate,
                    "offered_evals_per_s": sum(r.n_px * r.K for r in reqs) / reqs[-1].arrival})
@@ -725,7 +735,7 @@ def run_serve(args, rank, world, local, dev):
         if name == "served_bf16" and args.serve_serial_prefix > 0:
             m = args.serve_serial_prefix
             prefix = serve.make_stream(m, args.serve_rate, seed=rank, face_size=S)
-            st2 = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=12.0,
+            st2 = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=args.serve_quantum_ms,
                                       est_evals_per_s=rate).run(prefix)
             out["served_bf16_prefix"] = st2
             prefix = serve.make_stream(m, args.serve_rate, seed=rank, face_size=S)
@@ -734,14 +744,15 @@ def run_serve(args, rank, world, local, dev):
         del frames, base
         torch.cuda.empty_cache()
     if rank == 0:
-        s = out["served_bf16"]
+        s = out.get("served_bf16") or out["served_bf16_small_net"]
         line = {"metric": f"p99 relight latency, {args.serve_requests} requests Poisson {args.serve_rate:g}/s",
                 "value": s["p99_ms"], "unit": "ms", "n_gpus": world, "steps": 1, "warmup": 0,
                 "ms_per_step": s["makespan_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
                 "config": {"workload": "serving stream: resolutions {256^2, 512^2, 720p, 1080p, 1440p}, "
                                        "K in {64,128,300}, 40% new 6x64x64 env maps, 60% rotations, "
-                                       "150 GB admission budget, 12 ms quanta"},
+                                       f"150 GB admission budget, {args.serve_quantum_ms:g} ms quanta",
+                           "networks": args.serve_nets},
                 "clocks": clocks, **out}
         print(json.dumps(line), flush=True)
 
