@@ -11,13 +11,12 @@
 // Design, from measurements on B200: an M=128 N=64 tcgen05.mma issued back to back from an
 // elected lane of a converged warp takes ~36 cycles (~90% of the tensor peak), and five
 // independent 4-MMA layer chains saturate the pipe; issued from a lone lane of a diverged
-// warp the same MMAs take ~75 cycles, which cost this kernel 23%.  Keeping the activations
-// in shared memory made the kernel shared-memory-bandwidth bound (operand reads + epilogue
-// stores ~266 KB per tile and wavelet).  So activations live
-// in TMEM: the A operand of every layer is read by the MMA straight from tensor memory
-// (the ".kind::f16 [d], [a], b_desc" form), and the epilogue writes it back with a
-// single tcgen05.st.  Only the weights (B) and the per-tile aux block come from shared
-// memory.
+// warp the same MMAs take ~75 cycles.  Keeping the activations in shared memory made the
+// kernel shared-memory-bandwidth bound (operand reads + epilogue stores ~266 KB per tile and
+// wavelet).  So activations live in TMEM: the A operand of every layer is read by the MMA
+// straight from tensor memory (the ".kind::f16 [d], [a], b_desc" form), and the epilogue
+// writes it back with a single tcgen05.st.  Only the weights (B) and the per-tile aux block
+// come from shared memory; V_last, the FP32 output layer, comes from the kernel parameters.
 //
 // Organisation (one persistent CTA per SM): kNWG = 5 warpgroups, one 128-pixel tile each,
 // 96 TMEM columns per tile (480 of 512): [0,32) the BF16 A operand (2 values per 32-bit
@@ -25,17 +24,20 @@
 // epilogue round trips, and the kernel is bound by their latency, so five chains beat
 // four (640 threads leave ~96 registers each: the hash features of a tile live in shared
 // memory, and each half of an accumulator is packed and stored back before the next).
-// Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may access.  Per layer: wait on the tile's commit barrier -> tcgen05.ld
-// -> ReLU + cvt.rn.relu.bf16x2 -> tcgen05.st into the A columns -> warpgroup barrier
-// (bar.red.and carrying the "no timeout" vote) -> an elected lane of warp 0 issues the next
-// layer's MMAs and commits them.  The final layer's epilogue forms T_k, does the
-// clamped Kahan sum and writes the next wavelet's first-layer operand hash(p) * E_k+1.
-// Every wait is bounded by %globaltimer (2 s); on expiry the kernel records
-// kDevWaitTimeout and the warpgroup unwinds together.
+// Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may access.  Per
+// layer: wait on the tile's commit barrier -> tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 ->
+// tcgen05.st into the A columns -> warpgroup barrier (bar.red.and carrying the "no
+// timeout" vote) -> an elected lane of warp 0 issues the next layer's MMAs and commits
+// them.  The final layer's epilogue forms T_k, does the clamped Kahan sum and writes the
+// next wavelet's first-layer operand hash(p) * E_k+1.  The two standard networks run
+// kernels specialised on their layer sequence (ShapeOf), every other supported network a
+// generic form that reads the sequence from the plan.  Every wait is bounded by
+// %globaltimer (2 s); on expiry the kernel records kDevWaitTimeout and the warpgroup
+// unwinds together.
 #include <algorithm>
-#include <type_traits>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "nwprt_internal.cuh"
 
