@@ -188,7 +188,8 @@ class RelightServer:
     def __init__(self, engine, frames, base_faces, precision: str = "bf16", budget_bytes: int = 150 << 30,
                  quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
                  max_in_flight: int = 2, keep_outputs: bool = False,
-                 fault: Optional[Callable[[Request, str], Optional[str]]] = None):
+                 fault: Optional[Callable[[Request, str], Optional[str]]] = None,
+                 max_active: Optional[int] = None):
         import torch
         self.torch = torch
         self.e = engine
@@ -200,6 +201,8 @@ class RelightServer:
         self.quantum = int(est_evals_per_s * quantum_ms / 1e3)
         self.max_queue_s = max_queue_s
         self.max_in_flight = max_in_flight
+        # admission also stops at max_active admitted requests (None: the byte budget alone)
+        self.max_active_cap = max_active
         self.keep_outputs = keep_outputs
         self.fault = fault
         self.stream = torch.cuda.current_stream()
@@ -279,7 +282,7 @@ class RelightServer:
                 r.status = "queued"
                 queue.append(r)
             # admission (FCFS under the byte budget; over-budget and stale requests are refused)
-            while queue:
+            while queue and (self.max_active_cap is None or len(active) < self.max_active_cap):
                 r = queue[0]
                 try:
                     validate_request(r, len(self.frames), self.face_size, len(self.base_faces))
