@@ -133,6 +133,20 @@ def test_budget_admits_one_request_at_a_time(rig):
     assert stats["done"] == 6 and srv.max_active == 1
 
 
+def test_admission_cap_limits_concurrency_and_keeps_results(rig):
+    import torch
+    e, frames, base = rig
+    reqs = _requests(10, seed=5, spacing=0.0)
+    srv = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=0.05, est_evals_per_s=9e9,
+                              keep_outputs=True, max_active=2)
+    stats = srv.run(reqs)
+    assert stats["done"] == len(reqs), stats
+    assert srv.max_active <= 2
+    for r in reqs[:4]:
+        ind, _ = _solo(e, frames, base, r)
+        assert torch.equal(r.outputs[0], ind), r.rid
+
+
 def test_rejection_timeout_and_error_paths(rig):
     e, frames, base = rig
     reqs = _requests(5, seed=3, spacing=0.0)
