@@ -173,10 +173,9 @@ struct TcLayer {
 struct TcPlan {
   TcLayer layers[kMaxTcLayers];
   int n_layers = 0;
-  uint32_t vlast_off = 0;   // byte offset of V_last (FP32 [3][64]) in the blob
   uint32_t blob_bytes = 0;
   float cp_scale = 1.f;     // FP8: scale of the first layer's operand hash(p) * E_k
-  float vlast[3][64] = {};  // V_last as stored in the blob (filled when the weights are given)
+  float vlast[3][64] = {};  // V_last, FP32 [c][j] (filled when the weights are given)
 };
 enum TcMode { kTcBf16 = 0, kTcCalibrate = 1, kTcFp8 = 2 };
 bool relight_tc_supported(const NetDims& d, std::string* why);

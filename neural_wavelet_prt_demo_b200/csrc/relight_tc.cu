@@ -52,7 +52,6 @@ constexpr int kTmemCols = 512;
 constexpr int kTileCols = 96;              // TMEM columns per tile
 constexpr int kAcol = 0;                   // A operand columns [0, 32)
 constexpr int kDcol = 32;                  // accumulator columns [32, 96)
-constexpr int kVlastFloats = 3 * 64;
 constexpr uint64_t kWaitNs = 2000000000ull;
 // The job table travels inside the kernel parameters (sm_100 takes up to 32 KB): a launch
 // needs no host->device copy that could queue behind an unrelated bulk transfer.  Larger
@@ -65,7 +64,6 @@ struct TcParams {
   const float* hash;
   const uint4* wblob;
   uint32_t wblob_bytes;
-  uint32_t vlast_off;  // byte offset of V_last (FP32 [3][64]) in the blob
   TcLayer layers[kMaxTcLayers];
   int n_layers;
   int enc_dims;  // D, multiple of 16, <= 32
@@ -521,7 +519,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   using Sh = ShapeOf<SHAPE>;
   const int n_layers = SHAPE ? Sh::nl : p.n_layers;
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* wsm = smem;                                       // weight blob (+ V_last)
+  uint8_t* wsm = smem;                                       // weight blob
   uint8_t* aux = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kNWG][kAuxBytes]
   uint32_t* encs = reinterpret_cast<uint32_t*>(aux + kNWG * kAuxBytes);  // [kNWG][DMAX/2][kTile]
   TcBarriers* bars = reinterpret_cast<TcBarriers*>(encs + kNWG * (DMAX / 2) * kTile);
@@ -862,23 +860,14 @@ TcPlan make_plan(const NetDims& d, const float* op, const float* cn, int eb, con
     P.layers[P.n_layers++] = L;
   }
   P.layers[P.n_layers - 1].fin = 1;
-  // V_last: the 3 x 64 output layer in FP32, [c][j]
-  P.vlast_off = (uint32_t)off;
-  const size_t vbytes = kVlastFloats * 4;
-  if (blob) blob->resize(off + vbytes, 0);
+  // V_last: the 3 x 64 output layer in FP32, [c][j]; it travels in the kernel parameters
   if (fill) {
     const float* w = vlast_src(d, cn);
     const int n_in = d.cn_in[d.cn_nl - 1];
     const float inv = eb == 2 ? 1.f : 1.f / dscale[P.n_layers - 1];
     for (int c = 0; c < 3; ++c)
-      for (int j = 0; j < 64; ++j) {
-        const float v = j < n_in ? w[(size_t)c * n_in + j] * inv : 0.f;
-        std::memcpy(blob->data() + off + (c * 64 + j) * 4, &v, 4);
-        P.vlast[c][j] = v;
-      }
+      for (int j = 0; j < 64; ++j) P.vlast[c][j] = j < n_in ? w[(size_t)c * n_in + j] * inv : 0.f;
   }
-  off += vbytes;
-  off = (off + 127) & ~size_t(127);
   if (blob) blob->resize(off, 0);
   P.blob_bytes = (uint32_t)off;
   return P;
@@ -1025,7 +1014,6 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.hash = hash;
   p.wblob = reinterpret_cast<const uint4*>(blob_dev);
   p.wblob_bytes = P.blob_bytes;
-  p.vlast_off = P.vlast_off;
   std::memcpy(p.vlast, P.vlast, sizeof(p.vlast));
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
   p.n_layers = P.n_layers;
