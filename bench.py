@@ -57,6 +57,8 @@ def parse_args():
                     help="serve: kernel time per scheduling quantum")
     ap.add_argument("--serve-nets", choices=["both", "large", "small"], default="both",
                     help="serve: which network(s) to run (config 2, config 0, or both)")
+    ap.add_argument("--serve-order", choices=["fifo", "srpt"], default="fifo",
+                    help="serve: quantum packing order (arrival, or least remaining work)")
     ap.add_argument("--serve-max-active", type=int, default=0,
                     help="serve: admit at most this many requests at once (0: the byte budget alone)")
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
@@ -725,7 +727,7 @@ def run_serve(args, rank, world, local, dev):
         reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=rank, face_size=S)
         srv = serve.RelightServer(e, frames, base, precision="bf16", budget_bytes=150 << 30,
                                   quantum_ms=args.serve_quantum_ms, est_evals_per_s=rate,
-                                  max_active=args.serve_max_active or None)
+                                  max_active=args.serve_max_active or None, order=args.serve_order)
         first = clocks is None
         if first:
             sampler.start()

@@ -4,10 +4,11 @@ Requests of mixed resolution, K and env map arrive over time.  The server keeps 
 network weights and the G-buffers of every resolution resident in HBM, admits requests
 while a device-memory budget allows (their output buffers and env tables), and feeds the
 GPU fixed-size *quanta* of work: each quantum is one ``nwprt_relight_ranges`` launch that
-packs 128-pixel-aligned pixel ranges of several admitted requests, smallest remaining
-work first.  Requests that arrive while quanta are running join the next quantum, so
-large requests never block small ones for longer than one quantum, and two quanta are
-kept in flight so the GPU does not idle while the host forms the next one.
+packs 128-pixel-aligned pixel ranges of several admitted requests, in arrival order
+(``order="fifo"``, the default: it gives the lower p99) or smallest remaining work first
+(``order="srpt"``: lower p50 when the stream overloads the GPU).  Requests that arrive while
+quanta are running join the next quantum, and two quanta are kept in flight so the GPU does
+not idle while the host forms the next one.
 
 Each request's env map is either new cubemap faces (Haar + top-K on the GPU) or a
 rotation of a resident map (``env_rotate`` then Haar + top-K), stream-ordered ahead of
@@ -118,13 +119,17 @@ class Admission:
         assert self.used >= 0
 
 
-def plan_quantum(active: Sequence[Request], quantum_evals: int) -> List[Tuple[Request, int, int]]:
-    """Chunks for one launch: requests in order of least remaining work, each chunk a
-    128-pixel-aligned range, until the quantum is full.  Always makes progress: the first
-    request gets at least one tile even if that alone exceeds the quantum."""
+def plan_quantum(active: Sequence[Request], quantum_evals: int, order: str = "srpt") -> List[Tuple[Request, int, int]]:
+    """Chunks for one launch: requests in order of least remaining work ("srpt") or of
+    arrival ("fifo"), each chunk a 128-pixel-aligned range, until the quantum is full.
+    Always makes progress: the first request gets at least one tile even if that alone
+    exceeds the quantum."""
+    if order not in ("srpt", "fifo"):
+        raise ValueError(f"unknown quantum order {order!r}")
+    key = (lambda r: (r.remaining_evals, r.rid)) if order == "srpt" else (lambda r: (r.arrival, r.rid))
     plan = []
     used = 0
-    for r in sorted((r for r in active if r.next_px < r.n_px), key=lambda r: (r.remaining_evals, r.rid)):
+    for r in sorted((r for r in active if r.next_px < r.n_px), key=key):
         room = quantum_evals - used
         if room <= 0 and plan:
             break
@@ -189,7 +194,7 @@ class RelightServer:
                  quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
                  max_in_flight: int = 2, keep_outputs: bool = False,
                  fault: Optional[Callable[[Request, str], Optional[str]]] = None,
-                 max_active: Optional[int] = None):
+                 max_active: Optional[int] = None, order: str = "fifo"):
         import torch
         self.torch = torch
         self.e = engine
@@ -203,6 +208,7 @@ class RelightServer:
         self.max_in_flight = max_in_flight
         # admission also stops at max_active admitted requests (None: the byte budget alone)
         self.max_active_cap = max_active
+        self.order = order  # quantum packing order: "srpt" (least remaining work) or "fifo"
         self.keep_outputs = keep_outputs
         self.fault = fault
         self.stream = torch.cuda.current_stream()
@@ -319,7 +325,7 @@ class RelightServer:
                 active.append(r)
             self.max_active = max(self.max_active, len(active))
             if active and len(in_flight) < self.max_in_flight:
-                plan = plan_quantum(active, self.quantum)
+                plan = plan_quantum(active, self.quantum, self.order)
                 launch = []
                 for r, b, e in plan:
                     try:
