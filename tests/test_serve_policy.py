@@ -25,6 +25,18 @@ def test_quantum_is_tile_aligned_srpt_and_bounded():
     assert used <= q
 
 
+def test_quantum_fifo_order_follows_arrival():
+    active = [_req(0, 1920 * 1080, 300), _req(1, 256 * 256, 64), _req(2, 512 * 512, 128)]
+    for r, t in zip(active, (0.5, 0.2, 0.1)):
+        r.arrival = t
+    plan = serve.plan_quantum(active, 10 ** 12, order="fifo")
+    assert [r.rid for r, _, _ in plan] == [2, 1, 0]          # earliest arrival first
+    plan = serve.plan_quantum(active, 10 ** 12)
+    assert [r.rid for r, _, _ in plan] == [1, 2, 0]          # default: least remaining work first
+    with pytest.raises(ValueError):
+        serve.plan_quantum(active, 10 ** 12, order="lifo")
+
+
 def test_quantum_always_progresses_and_finishes_requests():
     r = _req(0, 1000, 300)
     plans = 0
