@@ -567,8 +567,8 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w8, &ctx->fp8_plan, mode, jobs.data(),
                       (int)jobs.size(), o.kahan, o.clamp_terms, nullptr, ctx->d_err, st);
   else
-    launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, &ctx->bf16_plan, mode, jobs.data(), (int)jobs.size(),
-                      o.kahan, o.clamp_terms, amax, ctx->d_err, st);
+    launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, &ctx->bf16_plan, mode, jobs.data(),
+                      (int)jobs.size(), o.kahan, o.clamp_terms, amax, ctx->d_err, st);
 }
 
 static void relight_ranges(nwprt_ctx* ctx, const std::vector<RangeReq>& reqs, const nwprt_relight_opts& o,

@@ -336,7 +336,8 @@ __device__ __forceinline__ void final_dot32x2(const uint32_t (&v)[32], const flo
 #pragma unroll
   for (int j2 = 0; j2 < 16; ++j2) {
     const int j = j0 + 2 * j2;
-    const unsigned long long h = pk2(fmaxf(__uint_as_float(v[2 * j2]), 0.f), fmaxf(__uint_as_float(v[2 * j2 + 1]), 0.f));
+    const unsigned long long h =
+        pk2(fmaxf(__uint_as_float(v[2 * j2]), 0.f), fmaxf(__uint_as_float(v[2 * j2 + 1]), 0.f));
     fma2(q0, pk2(V[0][j], V[0][j + 1]), h);
     fma2(q1, pk2(V[1][j], V[1][j + 1]), h);
     fma2(q2, pk2(V[2][j], V[2][j + 1]), h);
@@ -597,8 +598,9 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     tc_fence_before();
     fence_proxy_async_smem();
     ok = wg_barrier_and(g, ok);
-    if (ok && q == 0 && elect_one()) issue_layer<MODE>(p.layers[0], SHAPE ? Sh::aux == 0 : p.layers[0].aux != 0, wbase, a_tmem, aux_base, d_tmem,
-                                                        acc_bar);
+    if (ok && q == 0 && elect_one())
+      issue_layer<MODE>(p.layers[0], SHAPE ? Sh::aux == 0 : p.layers[0].aux != 0, wbase, a_tmem, aux_base, d_tmem,
+                        acc_bar);
     for (int k = 0; k < K && ok; ++k) {
 #pragma unroll(SHAPE ? Sh::nl : 1)
       for (int l = 0; l < n_layers; ++l) {
