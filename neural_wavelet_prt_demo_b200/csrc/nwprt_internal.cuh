@@ -140,7 +140,6 @@ struct DeviceWeights {
 };
 
 // relight_fp32.cu
-bool relight_fp32_supported(const NetDims& d, std::string* why);
 void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWeights& w,
                          const RelightJob& job, int clamp, int kahan, cudaStream_t st);
 // Host-side packing of FP32 weights into the kernel's transposed layout.

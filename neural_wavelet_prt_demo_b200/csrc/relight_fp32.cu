@@ -418,21 +418,6 @@ void pack_fp32_weights(const NetDims& d, const float* op, const float* cn, std::
 
 // The two standard shapes run compile-time kernels; every other network whose layers are at
 // most 64 wide (and whose weights fit in shared memory) runs the generic kernel.
-bool relight_fp32_supported(const NetDims& d, std::string* why) {
-  GenNet g;
-  if (!gen_net(d, &g, why)) return false;
-  int dev = 0, max_smem = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-    max_smem = 227 * 1024;
-  const int w_floats = (int)(d.n_op_params() + d.n_cn_params());  // lower bound of the padded size
-  if (gen_smem_bytes(g, w_floats, 128) > (size_t)max_smem) {
-    if (why) *why = "fp32 relight: network too large for shared memory";
-    return false;
-  }
-  return true;
-}
-
 void launch_relight_fp32(const NetDims& d, const HashLevels& hl, const DeviceWeights& w,
                          const RelightJob& job, int clamp, int kahan, cudaStream_t st) {
   if (job.n_px <= job.px_begin) return;
