@@ -39,10 +39,12 @@ def relight(case, precision="bf16", kahan=True, clamp=True):
     (netconfig.CONFIG_LARGE, 64, 40, 64, 1e-4),
     (netconfig.CONFIG_LARGE, 48, 30, 300, 1e-4),
     (netconfig.CONFIG_LARGE, 32, 20, 512, 1e-4),
+    (netconfig.CONFIG_LARGE, 16, 8, 1024, 1e-4),
     (netconfig.CONFIG_LARGE, 33, 17, 29, 0.5),
     (netconfig.CONFIG_SMALL, 128, 128, 64, 1e-4),
     (netconfig.CONFIG_SMALL, 31, 9, 17, 0.5),
-], ids=["large-k64", "large-k300", "large-k512", "large-ragged-hash", "small-config0", "small-ragged"])
+], ids=["large-k64", "large-k300", "large-k512", "large-k1024", "large-ragged-hash", "small-config0",
+       "small-ragged"])
 def test_bf16_psnr_vs_fp64(cuda, cfg, w, h, K, hs):
     case = make_case(cfg, w, h, K, seed=K, hash_scale=hs, flag_prob=0.9,
                      param_round="fp16" if cfg is netconfig.CONFIG_LARGE else "fp32")
