@@ -9,8 +9,11 @@
  *  - Device pointers are borrowed (caller-owned CUDA device memory) unless a
  *    parameter says "host".
  *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
- *    All work is stream-ordered on the caller's stream; nothing blocks the host
- *    except the calls documented as synchronous (load, env_get_wavelets, sync).
+ *    All work is stream-ordered on the caller's stream.  Calls that block the host:
+ *    nwprt_load_weights / _dir, nwprt_env_get_wavelets, nwprt_calibrate_fp8 and nwprt_sync;
+ *    nwprt_env_from_faces / nwprt_env_from_wavelets when their arrays are host memory
+ *    (they synchronise `stream` after the upload); nwprt_prepare when a frame grows beyond
+ *    the buffers it had (it synchronises the device before it frees them).
  *  - A context is bound to one device and is externally synchronised: one host
  *    thread at a time per context.
  *  - float4 buffers are 16-byte aligned arrays of 4 floats per pixel, row-major
@@ -253,18 +256,20 @@ NWPRT_API nwprt_status nwprt_sh_interpolate(nwprt_ctx* ctx, const float* vertex_
 NWPRT_API size_t nwprt_sh_project_workspace_size(int S);
 NWPRT_API nwprt_status nwprt_sh_project(const float* faces, int S, float* L, void* workspace,
                               size_t workspace_bytes, void* stream);
-/* Per-pixel SH dot product out[p] = (|sum_j T[p][j] L[j]|, 1) (float4 per pixel) -- the
- * light-vector product of __closesthit__SHradiance (device_functions/devicePrograms.cu:479-490)
- * for per-pixel transport vectors.  abs_out = 0 drops the abs of :490. */
 /* nwprt_sh_project without a workspace, for callers that cannot allocate device memory
  * (a frame loop that must never reach cudaMalloc/cudaFree, which can synchronise the device,
  * or a host that reserves all device memory up front).  No counterpart in the reference.
  * The partial sums live in a fixed static device array (373,248 bytes, held by every GPU
  * that loads the library until exit), so S must be <= 128.  The first call on a device
  * looks up that array's address with the device current; make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. */
+ * capture, and do not call cudaDeviceReset afterwards in the same process (the cached
+ * address would be stale).  Each device has its own array: calls that overlap on the same
+ * device (e.g. on two streams) race and must be serialised by the caller; calls on
+ * different devices do not race. */
 NWPRT_API nwprt_status nwprt_sh_project_static(const float* faces, int S, float* L, void* stream);
+/* Per-pixel SH dot product out[p] = (|sum_j T[p][j] L[j]|, 1) (float4 per pixel) -- the
+ * light-vector product of __closesthit__SHradiance (device_functions/devicePrograms.cu:479-490)
+ * for per-pixel transport vectors.  abs_out = 0 drops the abs of :490. */
 NWPRT_API nwprt_status nwprt_sh_dot(const float* T, int64_t n_px, int n_coeffs, const float* L,
                           int abs_out, float* out, void* stream);
 

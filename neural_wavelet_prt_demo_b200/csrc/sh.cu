@@ -21,9 +21,33 @@ namespace {
 
 constexpr int kLmax = 8;
 constexpr int kNc = (kLmax + 1) * (kLmax + 1);  // 81
-__constant__ float c_shK[kNc];                  // K(l,m) for m >= 0 at index l*l+l+m
 
 __host__ __device__ constexpr int shi(int l, int m) { return l * l + l + m; }
+
+// Normalisation K(l,m) = sqrt((2l+1)/(4 pi) * (l-m)!/(l+m)!) for m >= 0 at index l*l+l+m
+// (the pbrt-v2 basis, device_functions/shaderUtils.h:283-285).  The table is evaluated at
+// compile time (Newton's iteration for the square root, in double, then rounded once to
+// float: the same bits as the correctly rounded std::sqrt for all 45 entries), so it is part
+// of the module image and no call ever copies it to the device.
+constexpr double sqrt_newton(double x) {
+  double r = x > 1.0 ? x : 1.0;
+  for (int i = 0; i < 200; ++i) r = 0.5 * (r + x / r);
+  return r;
+}
+struct ShKTable {
+  float v[kNc];
+};
+constexpr ShKTable make_sh_k_table() {
+  ShKTable t{};
+  for (int l = 0; l <= kLmax; ++l)
+    for (int m = 0; m <= l; ++m) {
+      double ratio = 1.0;
+      for (int q = l - m + 1; q <= l + m; ++q) ratio /= (double)q;
+      t.v[shi(l, m)] = (float)sqrt_newton((2.0 * l + 1.0) / (4.0 * 3.14159265358979323846) * ratio);
+    }
+  return t;
+}
+__constant__ ShKTable c_shK = make_sh_k_table();
 
 __device__ __forceinline__ void sh_eval8(float x, float y, float z, float* Y) {
   float P[kNc];
@@ -57,10 +81,10 @@ __device__ __forceinline__ void sh_eval8(float x, float y, float z, float* Y) {
   const float sqrt2 = 1.41421356237309515f;
 #pragma unroll
   for (int l = 0; l <= kLmax; ++l) {
-    Y[shi(l, 0)] = c_shK[shi(l, 0)] * P[shi(l, 0)];
+    Y[shi(l, 0)] = c_shK.v[shi(l, 0)] * P[shi(l, 0)];
 #pragma unroll
     for (int m = 1; m <= l; ++m) {
-      const float kp = sqrt2 * c_shK[shi(l, m)] * P[shi(l, m)];
+      const float kp = sqrt2 * c_shK.v[shi(l, m)] * P[shi(l, m)];
       Y[shi(l, m)] = kp * cs[m];
       Y[shi(l, -m)] = kp * sn[m];
     }
@@ -124,18 +148,6 @@ __global__ void sh_project_reduce(const float* __restrict__ part, int n_blocks, 
     for (int b = 0; b < n_blocks; ++b) acc += part[(size_t)b * (kNc * 3) + tid];
     L[tid] = acc;
   }
-}
-
-bool upload_sh_constants() {
-  float K[kNc];
-  for (int l = 0; l <= kLmax; ++l)
-    for (int m = 0; m <= l; ++m) {
-      double ratio = 1.0;
-      for (int t = l - m + 1; t <= l + m; ++t) ratio /= (double)t;
-      K[shi(l, m)] = (float)std::sqrt((2.0 * l + 1.0) / (4.0 * M_PI) * ratio);
-      if (m > 0) K[shi(l, -m)] = 0.f;
-    }
-  return cudaMemcpyToSymbol(c_shK, K, sizeof(K)) == cudaSuccess;
 }
 
 // ------------------------------------------------------------------ sh_dot
@@ -223,13 +235,6 @@ size_t sh_project_workspace_bytes(int S) {
 }
 
 void launch_sh_project(const float* faces, int S, float* L, float* workspace, cudaStream_t st) {
-  static thread_local int uploaded_dev = -1;
-  int dev = 0;
-  NWPRT_CUDA(cudaGetDevice(&dev));
-  if (uploaded_dev != dev) {
-    if (!upload_sh_constants()) fail(NWPRT_CUDA_ERROR, "sh_project: constant upload failed");
-    uploaded_dev = dev;
-  }
   const long long n = 6LL * S * S;
   const int blocks = (int)((n + kProjThreads - 1) / kProjThreads);
   const size_t smem = sizeof(float) * (kNc + 3) * kProjPad;

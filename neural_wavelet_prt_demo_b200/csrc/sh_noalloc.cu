@@ -11,11 +11,14 @@
 // Host code never uses the array's name as a device address (in host code that name is
 // only a host-side stand-in).  Instead, the first call on each device, with that device
 // current, looks up the array's device address with cudaGetSymbolAddress and caches it;
-// that first call should therefore come before any stream capture.  All calls share the
-// one array and it keeps the previous call's contents: every partial sum a call reads
-// is written earlier in the same call, so nothing needs clearing, but calls whose work
-// overlaps on the GPU (different streams, or devices sharing nothing else) race on it
-// and must be serialised by the caller.
+// that first call should therefore come before any stream capture.  The cached address
+// belongs to the device's current primary context: a host application that calls
+// cudaDeviceReset after using this entry point must not call it again in that process.
+// Every device holds its own instance of the array.  All calls on one device share that
+// instance and it keeps the previous call's contents: every partial sum a call reads is
+// written earlier in the same call, so nothing needs clearing, but calls that overlap on
+// the same device (for example on two streams) race on it and must be serialised by the
+// caller.  Calls on different devices do not race.
 #include <mutex>
 
 #include "nwprt_internal.cuh"

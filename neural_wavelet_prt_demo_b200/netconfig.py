@@ -5,7 +5,7 @@ The reference builds its network from ``config_comp.json`` with the four keys
 (Renderer/tinycudann/prt_network.h:38-61).  That JSON and the tiny-cuda-nn
 factories it feeds are not shipped with the reference, so this module pins the
 meaning of every key we accept.  The same JSON text is parsed by the native
-library (``csrc/nwprt_config.cpp``) and by the CPU oracle driver; both derive
+library (``csrc/config.cpp``) and by the CPU oracle driver; both derive
 the same numbers from it with the formulas below.
 
 Composite network (prt_network.h:73-154), per pixel p and selected wavelet k:

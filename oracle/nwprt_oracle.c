@@ -583,12 +583,12 @@ static int net_ok(const orc_net* net) {
   return 1;
 }
 
-static void transport_f32_t(const orc_net* net, const orc_weights* w, const float* op_t,
-                            const float* cn_t, const orc_gbuf* g, int64_t px, const int32_t* idx,
-                            int K, float* out) {
-  float row[16], enc[ORC_MAX_WIDTH], aux[ORC_MAX_WIDTH];
+/* Transport of one pixel from its 16-float input row (the layout of prt_globals.h:4-13). */
+static void transport_f32_row(const orc_net* net, const orc_weights* w, const float* op_t,
+                              const float* cn_t, const float row[16], const int32_t* idx, int K,
+                              float* out) {
+  float enc[ORC_MAX_WIDTH], aux[ORC_MAX_WIDTH];
   float xa[ORC_MAX_WIDTH], xb[ORC_MAX_WIDTH];
-  orc_remap_f32(g, px, row);
   orc_hash_encode_f32(net, w->hash, row, enc);
   for (int i = 0; i < net->aux_width; ++i) aux[i] = i < 13 ? row[3 + i] : 1.0f;
   const int D = net->n_levels * net->n_features;
@@ -611,6 +611,14 @@ static void transport_f32_t(const orc_net* net, const orc_weights* w, const floa
     }
     out[k * 3 + 0] = x[0]; out[k * 3 + 1] = x[1]; out[k * 3 + 2] = x[2];
   }
+}
+
+static void transport_f32_t(const orc_net* net, const orc_weights* w, const float* op_t,
+                            const float* cn_t, const orc_gbuf* g, int64_t px, const int32_t* idx,
+                            int K, float* out) {
+  float row[16];
+  orc_remap_f32(g, px, row);
+  transport_f32_row(net, w, op_t, cn_t, row, idx, K, out);
 }
 
 int orc_transport_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g, int64_t px,
@@ -668,10 +676,10 @@ int orc_transport_f64(const orc_net* net, const orc_weights* w, const orc_gbuf* 
 /* Radiance sum of computeResponse (utils_kernels.h:52-91): only pixels whose
  * env-map flag is set get sum_k max(L_k * T_k, 0); indirect = (rgb, 1),
  * with_direct = (rgb + direct.rgb, 1). */
-int orc_relight_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
-                    const int32_t* idx, const float* strength, int K, int clamp, int kahan,
-                    int64_t px_begin, int64_t px_end, int n_threads,
-                    float* indirect4, float* with_direct4) {
+static int relight_f32_impl(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
+                            const float* rows, const int32_t* idx, const float* strength, int K,
+                            int clamp, int kahan, int64_t px_begin, int64_t px_end, int n_threads,
+                            float* indirect4, float* with_direct4) {
   if (!net_ok(net) || K < 0) return -1;
   int bad = 0;
   set_threads(n_threads);
@@ -684,7 +692,10 @@ int orc_relight_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
     for (int64_t p = px_begin; p < px_end; ++p) {
       float s[3] = {0.f, 0.f, 0.f}, comp[3] = {0.f, 0.f, 0.f};
       if (g->flag[p]) {
-        transport_f32_t(net, w, op_t, cn_t, g, p, idx, K, T);
+        if (rows)
+          transport_f32_row(net, w, op_t, cn_t, rows + (p - px_begin) * 16, idx, K, T);
+        else
+          transport_f32_t(net, w, op_t, cn_t, g, p, idx, K, T);
         for (int k = 0; k < K; ++k)
           for (int c = 0; c < 3; ++c) {
             float term = strength[k * 3 + c] * T[k * 3 + c];
@@ -711,6 +722,23 @@ int orc_relight_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
   free(op_t);
   free(cn_t);
   return bad ? -1 : 0;
+}
+
+int orc_relight_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
+                    const int32_t* idx, const float* strength, int K, int clamp, int kahan,
+                    int64_t px_begin, int64_t px_end, int n_threads,
+                    float* indirect4, float* with_direct4) {
+  return relight_f32_impl(net, w, g, NULL, idx, strength, K, clamp, kahan, px_begin, px_end,
+                          n_threads, indirect4, with_direct4);
+}
+
+int orc_relight_rows_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
+                         const float* rows, const int32_t* idx, const float* strength, int K,
+                         int clamp, int kahan, int64_t px_begin, int64_t px_end, int n_threads,
+                         float* indirect4, float* with_direct4) {
+  if (!rows) return -1;
+  return relight_f32_impl(net, w, g, rows, idx, strength, K, clamp, kahan, px_begin, px_end,
+                          n_threads, indirect4, with_direct4);
 }
 
 int orc_relight_f64(const orc_net* net, const orc_weights* w, const orc_gbuf* g,

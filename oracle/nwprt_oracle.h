@@ -102,6 +102,14 @@ int orc_relight_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
                     const int32_t* idx, const float* strength, int K, int clamp, int kahan,
                     int64_t px_begin, int64_t px_end, int n_threads,
                     float* indirect4, float* with_direct4);
+/* orc_relight_f32 with the per-pixel input rows given instead of remapped from the G-buffer:
+ * rows[(px - px_begin) * 16 + c] in the layout of prt_globals.h:4-13 (the flag and the direct
+ * light still come from g).  Feeds the reference's own waveletDataCopy rows
+ * (utils_kernels.h:7-49, built from oracle/_ref) through the same network. */
+int orc_relight_rows_f32(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
+                         const float* rows, const int32_t* idx, const float* strength, int K,
+                         int clamp, int kahan, int64_t px_begin, int64_t px_end, int n_threads,
+                         float* indirect4, float* with_direct4);
 int orc_relight_f64(const orc_net* net, const orc_weights* w, const orc_gbuf* g,
                     const int32_t* idx, const float* strength, int K, int clamp,
                     int64_t px_begin, int64_t px_end, int n_threads, double* rgb3);

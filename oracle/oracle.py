@@ -291,6 +291,25 @@ def relight_f32(b: Bound, idx, strength, clamp=True, kahan=True, px_begin=0, px_
     return ind, wd
 
 
+def relight_rows_f32(b: Bound, rows, idx, strength, px_begin, clamp=True, kahan=True, n_threads=0):
+    """relight_f32 over pixels [px_begin, px_begin + len(rows)) with the 16-float input rows
+    given (e.g. the reference's own waveletDataCopy rows) instead of remapped here."""
+    rows = np.ascontiguousarray(rows, np.float32).reshape(-1, 16)
+    idx = np.ascontiguousarray(idx, np.int32)
+    st = np.ascontiguousarray(strength, np.float32)
+    K = idx.shape[0]
+    px_end = px_begin + rows.shape[0]
+    ind = np.zeros((b.n_px, 4), np.float32)
+    wd = np.zeros((b.n_px, 4), np.float32)
+    rc = lib().orc_relight_rows_f32(C.byref(b.net), C.byref(b.w), C.byref(b.g), _p(rows), _p(idx),
+                                    _p(st), C.c_int(K), C.c_int(int(clamp)), C.c_int(int(kahan)),
+                                    C.c_int64(px_begin), C.c_int64(px_end), C.c_int(n_threads),
+                                    _p(ind), _p(wd))
+    if rc != 0:
+        raise ValueError("orc_relight_rows_f32 failed")
+    return ind, wd
+
+
 def relight_f64(b: Bound, idx, strength, clamp=True, px_begin=0, px_end=None, n_threads=0):
     idx = np.ascontiguousarray(idx, np.int32)
     st = np.ascontiguousarray(strength, np.float32)
@@ -312,6 +331,7 @@ def max_threads() -> int:
 # ---------------------------------------------------------------- reference kernels (host)
 
 def ref_wavelet_data_copy(gb):
+    """prt::waveletDataCopy of the reference (host build): [N, WAVELETNUM, 16] rows."""
     r = ref_lib()
     n = gb.width * gb.height
     K = r.ref_wavelet_num()

@@ -57,3 +57,22 @@ def bits_equal(a, b) -> bool:
     if not np.array_equal(na, nb):
         return False
     return bool(np.array_equal(a[~na].view(np.uint32), b[~nb].view(np.uint32)))
+
+
+def err_stats(x, ref, floor_frac=1e-6) -> dict:
+    """Error of an image against its reference, as every accuracy report states it:
+    max / mean relative error with denominators floored at ``floor_frac`` of the image
+    maximum, PSNR over the image maximum, and the largest absolute error as a fraction of
+    that maximum (the per-pixel bound that near-zero channels do not inflate)."""
+    x = np.asarray(x, np.float64)
+    ref = np.asarray(ref, np.float64)
+    mx, mean = rel_err(x, ref, floor_frac)
+    peak = float(np.abs(ref).max())
+    return {"max_rel_err": mx, "mean_rel_err": mean, "psnr_db": psnr(x, ref),
+            "max_abs_err_over_peak": float(np.abs(x - ref).max()) / peak if peak > 0 else 0.0}
+
+
+def load_golden(name):
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz")
+    return dict(np.load(path))

@@ -50,6 +50,39 @@ def test_static_projection_matches_workspace_projection_on_consecutive_calls(cud
         assert np.allclose(got, ref, rtol=1e-5, atol=1e-7 * float(np.abs(ref).max()))
 
 
+def test_static_projection_allocates_nothing(cuda):
+    """After a first call (which loads the module and looks up the array's address), further
+    calls leave the device's free memory unchanged: the partial sums never need an
+    allocation, which is what callers that cannot allocate rely on.  S = 100 also checks a
+    face size that is not a power of two, and a call from a new host thread checks that no
+    per-thread set-up is needed."""
+    import threading
+    import torch
+    from neural_wavelet_prt_demo_b200 import _lib
+    lib = _lib.lib()
+    S = 100
+    faces = torch.from_numpy(synth.make_env_faces(S, seed=21)).to(cuda)
+    s_ref, L_ref = _project_with_workspace(lib, faces, S)
+    assert s_ref == _lib.OK
+    L = torch.full((81, 3), float("nan"), dtype=torch.float32, device=cuda)
+    args = (C.c_void_p(faces.data_ptr()), S, C.c_void_p(L.data_ptr()), None)
+    assert lib.nwprt_sh_project_static(*args) == _lib.OK
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert lib.nwprt_sh_project_static(*args) == _lib.OK
+    statuses = []
+    t = threading.Thread(target=lambda: statuses.append(lib.nwprt_sh_project_static(*args)))
+    t.start()
+    t.join()
+    assert statuses == [_lib.OK]
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before, (free_before, free_after)
+    got, ref = L.cpu().numpy(), L_ref.cpu().numpy()
+    assert np.allclose(got, ref, rtol=1e-5, atol=1e-7 * float(np.abs(ref).max()))
+
+
 def test_static_projection_rejects_faces_beyond_its_scratch(cuda):
     import torch
     from neural_wavelet_prt_demo_b200 import _lib
