@@ -21,6 +21,7 @@ from __future__ import annotations
 import ctypes as C
 import json
 import os
+import re
 from dataclasses import dataclass, field
 from typing import List, Optional
 
@@ -106,6 +107,94 @@ class FullFrame:
                                              "fbDirectDenoised", "fbEnvironmentMapFlag")])
 
 
+def read_hdr(path: str) -> np.ndarray:
+    """Radiance RGBE image -> float32 [h, w, 3], rows in file order (top first).
+
+    "#?RADIANCE" signature, header lines up to an empty line, a "-Y <h> +X <w>" resolution
+    line, then h scanlines: run-length encoded per component (marker 2, 2, w // 256, w % 256;
+    count > 128 = a run of count - 128 copies, else count literal bytes) or flat RGBE
+    quadruples where (1, 1, 1, n) repeats the previous pixel n << shift times.  A channel
+    is mantissa / 256 * 2^(E - 128), as the reference converts it (HDRloader.cpp:108-125)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if not data.startswith(b"#?RADIANCE"):
+        raise RuntimeError(f"not a Radiance .hdr file: {path}")
+    pos = data.index(b"\n") + 1
+    while True:
+        end = data.find(b"\n", pos)
+        if end < 0:
+            raise RuntimeError(f"truncated .hdr header: {path}")
+        line, pos = data[pos:end], end + 1
+        if not line:
+            break
+    end = data.find(b"\n", pos)
+    m = re.match(rb"-Y (\d+) \+X (\d+)$", data[pos:end] if end >= 0 else b"")
+    if not m or int(m.group(1)) < 1 or int(m.group(2)) < 1:
+        raise RuntimeError(f"unsupported .hdr resolution line: {path}")
+    h, w = int(m.group(1)), int(m.group(2))
+    pos = end + 1
+    buf = np.frombuffer(data, np.uint8)
+    n_buf = buf.shape[0]
+    px = np.zeros((h, w, 4), np.uint8)
+
+    def take(n):
+        nonlocal pos
+        if pos + n > n_buf:
+            raise RuntimeError(f"truncated .hdr data: {path}")
+        pos += n
+        return buf[pos - n:pos]
+
+    for y in range(h):
+        q = take(4)
+        if 8 <= w <= 0x7FFF and q[0] == 2 and q[1] == 2 and not (q[2] & 0x80):
+            if (int(q[2]) << 8 | int(q[3])) != w:
+                raise RuntimeError(f".hdr scanline width mismatch: {path}")
+            for c in range(4):
+                x = 0
+                while x < w:
+                    n = int(take(1)[0])
+                    if n > 128:
+                        n -= 128
+                        if x + n > w:
+                            raise RuntimeError(f".hdr run overflows its scanline: {path}")
+                        px[y, x:x + n, c] = take(1)[0]
+                    else:
+                        if n == 0 or x + n > w:
+                            raise RuntimeError(f"bad .hdr dump: {path}")
+                        px[y, x:x + n, c] = take(n)
+                    x += n
+        else:
+            x, shift, first = 0, 0, True
+            while x < w:
+                if not first:
+                    q = take(4)
+                first = False
+                if q[0] == 1 and q[1] == 1 and q[2] == 1:
+                    n = int(q[3]) << shift
+                    if x == 0 or x + n > w:
+                        raise RuntimeError(f"bad .hdr repeat code: {path}")
+                    px[y, x:x + n] = px[y, x - 1]
+                    x += n
+                    shift += 8
+                else:
+                    px[y, x] = q
+                    x += 1
+                    shift = 0
+    scale = np.ldexp(np.float32(1.0), px[..., 3].astype(np.int32) - 128).astype(np.float32)
+    return (px[..., :3].astype(np.float32) / np.float32(256.0)) * scale[..., None]
+
+
+def _load_sh(path: str) -> np.ndarray:
+    """SH coefficients [(l+1)^2, 3] (Environment_Map::load_sh, EnvironmentMap.cpp:70-77)."""
+    a = np.load(path)
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise RuntimeError(f"SH .npy must be [n, 3]: {path}")
+    l = int(round(np.sqrt(a.shape[0]))) - 1
+    if (l + 1) ** 2 != a.shape[0]:
+        raise RuntimeError(f"SH .npy must hold (l+1)^2 rows: {path}")
+    return a.astype(np.float32)
+
+
 class EnvironmentMap:
     """Environment_Map (EnvironmentMap.h:11-40): cubemap faces and their wavelet table.
 
@@ -126,29 +215,54 @@ class EnvironmentMap:
 
     @staticmethod
     def cross_to_faces(cross: np.ndarray, from_npy: bool = True) -> np.ndarray:
-        """4x3 cross image [3S, 4S, 3] -> faces (EnvironmentMap.cpp:80-126).
-        ``.npy`` crosses are flipped vertically first, as loadCubeMap does (:96-101)."""
+        """4x3 cross image [3S, 4S, 3], rows as stored in the file (top first) -> faces
+        [6, S, S, 3] (EnvironmentMap.cpp:80-126).  The rows are flipped first: the reference
+        keeps both .npy crosses (:96-101) and .hdr crosses (HDRLoaderResult::get,
+        Renderer/HDRloader.h:21-25) bottom row first.  ``from_npy=False`` takes an image
+        that is already bottom row first."""
         img = np.asarray(cross, np.float32)
+        if img.ndim != 3 or img.shape[2] != 3:
+            raise ValueError("cross image must be [3S, 4S, 3]")
         if from_npy:
             img = img[::-1]
         S = img.shape[0] // 3
-        if img.shape[1] != 4 * S:
+        if S < 1 or img.shape[0] != 3 * S or img.shape[1] != 4 * S:
             raise ValueError("cross image must be 3S x 4S")
         # get_submatrix(from_c, from_r, ...) offsets in face units, initCubeFaces order
         cells = [(2, 1), (0, 1), (1, 2), (1, 0), (1, 1), (3, 1)]
         return np.stack([img[r * S:(r + 1) * S, c * S:(c + 1) * S] for c, r in cells]).copy()
 
     @staticmethod
+    def from_file(inFileName: str, sh_coeff: bool = False) -> "EnvironmentMap":
+        """Environment_Map(inFileName, sh_coeff) (EnvironmentMap.cpp:10-18): a 4x3 cross
+        cubemap in a .hdr or .npy file, or, with ``sh_coeff``, SH coefficients (.npy [n, 3])."""
+        if sh_coeff:
+            return EnvironmentMap(sh_coefficients=_load_sh(inFileName))
+        if not os.path.exists(inFileName):
+            raise RuntimeError("Invalid Env map File Name")
+        ext = os.path.splitext(inFileName)[1]
+        if ext == ".hdr":
+            img = read_hdr(inFileName)
+        elif ext == ".npy":
+            img = np.load(inFileName)
+            if img.dtype != np.float32:
+                raise RuntimeError(f"{inFileName} must hold float32 data")
+        else:
+            raise RuntimeError("Unknown type " + ext)
+        return EnvironmentMap(EnvironmentMap.cross_to_faces(img))
+
+    @staticmethod
     def from_folder(folder: str, name: str) -> "EnvironmentMap":
-        """Environment_Map(envMapFolder, envMapName) for .npy assets: cube/<name>.npy,
-        waveletcoeffs/<name>.npy, waveletstrength/<name>.npy, sh/<name>.npy (EnvironmentMap.cpp:20-68)."""
+        """Environment_Map(envMapFolder, envMapName) (EnvironmentMap.cpp:20-68): cube/<name>.hdr
+        (required), then sh/<name>.npy and the waveletcoeffs/<name>.npy +
+        waveletstrength/<name>.npy pair when present.  The latlong map feeds the reference's
+        direct-light shader only and is not read."""
         if not os.path.isdir(folder):
             raise RuntimeError("Invalid Env map Folder Name, it should not be a file")
-        cube = os.path.join(folder, "cube", name + ".npy")
+        cube = os.path.join(folder, "cube", name + ".hdr")
         if not os.path.exists(cube):
             raise RuntimeError("Invalid Env map File Name")
-        faces = EnvironmentMap.cross_to_faces(np.load(cube), from_npy=True)
-        em = EnvironmentMap(faces)
+        em = EnvironmentMap(EnvironmentMap.cross_to_faces(read_hdr(cube)))
         wc = os.path.join(folder, "waveletcoeffs", name + ".npy")
         ws = os.path.join(folder, "waveletstrength", name + ".npy")
         if os.path.exists(wc) and os.path.exists(ws):
@@ -159,7 +273,7 @@ class EnvironmentMap:
             em.topWaveletStrength = np.ascontiguousarray(st, np.float32)
         sh = os.path.join(folder, "sh", name + ".npy")
         if os.path.exists(sh):
-            em.shCoefficients = np.load(sh).astype(np.float32)
+            em.shCoefficients = _load_sh(sh)
         return em
 
     def computeWavelets(self, K: int, device="cuda:0") -> None:

@@ -76,3 +76,48 @@ def load_golden(name):
     import os
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz")
     return dict(np.load(path))
+
+
+def rgbe_encode(img):
+    """float [h, w, 3] -> RGBE bytes [h, w, 4]: exponent from the largest channel, mantissas
+    truncated (integers below 256 are stored exactly)."""
+    img = np.asarray(img, np.float64)
+    m = img.max(axis=-1)
+    frac, e = np.frexp(m)
+    live = m > 1e-38
+    scale = np.ldexp(1.0, np.where(live, 8 - e, 0))
+    mant = np.where(live[..., None], np.clip(np.floor(img * scale[..., None]), 0, 255), 0)
+    expo = np.where(live, e + 128, 0)
+    return np.concatenate([mant, expo[..., None]], axis=-1).astype(np.uint8)
+
+
+def write_hdr(path, img, rle=True):
+    """Radiance .hdr writer: run-length encoded scanlines (runs of >= 3 equal bytes, else
+    literal dumps) or flat RGBE quadruples."""
+    h, w, _ = np.asarray(img).shape
+    px = rgbe_encode(img)
+    out = bytearray(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {h} +X {w}\n".encode())
+    for y in range(h):
+        if not rle:
+            out += px[y].tobytes()
+            continue
+        out += bytes([2, 2, w >> 8, w & 255])
+        for c in range(4):
+            comp = px[y, :, c]
+            x = 0
+            while x < w:
+                n = 1
+                while x + n < w and comp[x + n] == comp[x] and n < 127:
+                    n += 1
+                if n >= 3:
+                    out += bytes([128 + n, comp[x]])
+                    x += n
+                else:
+                    m = 1
+                    while (x + m < w and m < 128
+                           and not (x + m + 2 < w and comp[x + m] == comp[x + m + 1] == comp[x + m + 2])):
+                        m += 1
+                    out += bytes([m]) + comp[x:x + m].tobytes()
+                    x += m
+    with open(path, "wb") as f:
+        f.write(bytes(out))
