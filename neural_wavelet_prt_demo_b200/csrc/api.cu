@@ -353,6 +353,7 @@ nwprt_status nwprt_load_weights(nwprt_ctx* ctx, const nwprt_weights* w) {
     if (ctx->tc_supported) {
       std::vector<uint16_t> tw;
       ctx->bf16_plan = pack_tc_weights(d, w->out_prd, w->cmp_net, &tw);
+      tw.resize(tc_blob_alloc_bytes(tw.size() * 2) / 2, 0);  // whole rows of the kernel's TMA view
       ctx->d_tc_w = dev_alloc<uint16_t>(tw.size());
       NWPRT_CUDA(cudaMemcpy(ctx->d_tc_w, tw.data(), tw.size() * 2, cudaMemcpyHostToDevice));
     }
@@ -663,6 +664,7 @@ nwprt_status nwprt_calibrate_fp8(nwprt_ctx* ctx, int env_id, int frame_id, int64
       std::memcpy(am.data(), bits.data(), am.size() * 4);
       std::vector<uint8_t> blob;
       TcPlan plan = pack_tc_weights_fp8(ctx->dims, ctx->h_op.data(), ctx->h_cn.data(), am.data(), &blob);
+      blob.resize(tc_blob_alloc_bytes(blob.size()), 0);  // whole rows of the kernel's TMA view
       // no launch may still read the previous blob
       NWPRT_CUDA(cudaDeviceSynchronize());
       dev_free(ctx->d_tc_w8);

@@ -9,15 +9,26 @@
 //  * key = |0.212671 r + 0.715160 g + 0.072169 b| (EnvironmentMap.cpp:149-151), NaN -> 0;
 //  * order = key descending, flat index face*S*S + row*S + col ascending.
 //
-// Design: a cluster of 6 CTAs (one per face) keeps every face in its own shared
-// memory: one bulk copy brings the face in, and every Haar level runs in place (operands
-// to registers, barrier, results back).  The top-K threshold is found by a 4-pass 8-bit
-// radix select: each CTA histograms its face, the cluster totals are summed through
-// distributed shared memory (the six remote loads issued together), and every CTA scans
-// the totals redundantly, so a pass costs one cluster barrier.  Ties at the threshold are
-// taken in flat-index order (one ordered block scan over the tie flags); the winners are
-// written into CTA 0's shared memory and ranked there.  Nothing but the inputs and
-// outputs touches global memory.
+// Design: a cluster of 6 CTAs (one per face) of 256 threads.  Nothing but the inputs and
+// outputs touches global memory, and the face never goes through shared memory:
+//  * Haar in registers.  Thread t owns the 4x4 texel block at block coordinates
+//    (bi, bj) = Morton(t) (bj on the even bits) and evaluates the first two levels on it
+//    alone: 15 detail coefficients stay in its registers, one LL value moves on.  Because
+//    the LL grid is held in Morton order, every 2x2 block of the next level sits in 4
+//    consecutive lanes and the next 16 in one warp, so two more levels are warp shuffles.
+//    The (at most 16) LL values left go through shared memory to warp 0, which finishes
+//    the last levels the same way: one block barrier for the whole transform.  The
+//    coefficients of those upper levels fill exactly the top-left (S/4)^2 block of the
+//    face, one per thread, so each thread owns 16 coefficients.
+//  * 4-pass 8-bit radix select of the K-th largest key over the cluster: each CTA
+//    histograms its keys (registers -> shared atomics), the six histograms are summed
+//    through distributed shared memory after one cluster barrier, and one block scan over
+//    the totals (thread t = digit 255 - t) finds the digit.
+//  * Ties at the threshold are ranked by flat index with a per-face bitmap and popcount
+//    prefixes; the per-face tie counts come from the last pass's histograms.
+//  * Winners get slots from one counter in CTA 0 (one atomic per warp) and are written to
+//    all six CTAs, so each CTA ranks a sixth of them (one warp per winner) and writes
+//    their outputs.
 #include <cooperative_groups.h>
 
 #include "nwprt_internal.cuh"
@@ -27,57 +38,57 @@ namespace cg = cooperative_groups;
 namespace nwprt {
 namespace {
 
-constexpr int kThreads = 512;
+constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxS = 64;
 constexpr int kMaxK = 1024;
-constexpr int kMaxPerThread = kMaxS * kMaxS / kThreads;            // keys per thread in the compaction
-constexpr int kMaxLevelQuads = (kMaxS / 2) * (kMaxS / 2) / kThreads;  // 2x2 Haar blocks per thread
 
-struct Gathered {
+struct Winner {
   float r, g, b;
   int32_t idx;
 };
 
 struct HaarSmem {
-  float* C;         // [S][S][3] the face, then its coefficients (in place)
-  uint32_t* keys;   // [S*S]
-  uint32_t* hist;   // [2][256] this face's histogram of the pass (double buffered)
-  uint32_t* all_h;  // [6][256] the cluster's histograms of the pass
-  uint32_t* tot;    // [256] their sum
-  uint64_t* gkey;   // [K] composite keys (CTA 0)
-  Gathered* gval;   // [K]
-  int* warp_tot;    // [kWarps]
-  int* scal;        // scalars
-  uint64_t* bar;    // bulk-copy completion
+  uint32_t* hist;    // [2][256] this face's histogram of the pass (double buffered)
+  float* upper;      // [(S/4)^2][3] coefficients of the top-left (S/4)^2 block
+  float* llg;        // [16][3] LL values handed to warp 0 for the last levels
+  uint32_t* bits;    // [S*S/32] ties at the threshold, by flat index within the face
+  uint32_t* wpre;    // [S*S/32] exclusive popcount prefix of `bits`
+  uint64_t* gkey;    // [K] composite keys of the winners (every CTA holds all of them)
+  Winner* gval;      // [K]
+  int* warp_tot;     // [kWarps]
+  int* scal;         // scalars
 };
+
+// scal[] slots
+constexpr int kScPrefix = 0, kScMask = 1, kScRemaining = 2, kScCounter = 3, kScEq = 8;  // eq: [6]
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 __host__ __device__ inline size_t smem_layout(int S, int K, char* base, HaarSmem* L) {
+  const int G = S < 4 ? 1 : S / 4;
+  const int nw = (S * S + 31) / 32;
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t at = o; o = align16(o + bytes); return at; };
-  size_t oC = take(sizeof(float) * S * S * 3);
-  size_t oK = take(sizeof(uint32_t) * S * S);
   size_t oH = take(sizeof(uint32_t) * 512);
-  size_t oA = take(sizeof(uint32_t) * 6 * 256);
-  size_t oT = take(sizeof(uint32_t) * 256);
+  size_t oU = take(sizeof(float) * 3 * G * G);
+  size_t oL = take(sizeof(float) * 3 * 16);
+  size_t oB = take(sizeof(uint32_t) * nw);
+  size_t oP = take(sizeof(uint32_t) * nw);
   size_t oG = take(sizeof(uint64_t) * K);
-  size_t oV = take(sizeof(Gathered) * K);
+  size_t oV = take(sizeof(Winner) * K);
   size_t oW = take(sizeof(int) * kWarps);
   size_t oS = take(sizeof(int) * 32);
-  size_t oB = take(sizeof(uint64_t));
   if (L) {
-    L->C = (float*)(base + oC);
-    L->keys = (uint32_t*)(base + oK);
     L->hist = (uint32_t*)(base + oH);
-    L->all_h = (uint32_t*)(base + oA);
-    L->tot = (uint32_t*)(base + oT);
+    L->upper = (float*)(base + oU);
+    L->llg = (float*)(base + oL);
+    L->bits = (uint32_t*)(base + oB);
+    L->wpre = (uint32_t*)(base + oP);
     L->gkey = (uint64_t*)(base + oG);
-    L->gval = (Gathered*)(base + oV);
+    L->gval = (Winner*)(base + oV);
     L->warp_tot = (int*)(base + oW);
     L->scal = (int*)(base + oS);
-    L->bar = (uint64_t*)(base + oB);
   }
   return o;
 }
@@ -101,260 +112,353 @@ __device__ __forceinline__ uint32_t wavelet_key_bits(float r, float g, float b) 
   return __float_as_uint(t);
 }
 
-// Exclusive prefix of `v` over the block's threads in thread order, plus the block total.
-__device__ __forceinline__ int block_exclusive_sum(int v, int* warp_tot, int* total) {
+// Bits 0, 2, 4, 6 of x packed into bits 0..3 (Morton decode of one coordinate).
+__device__ __forceinline__ int morton_even(int x) {
+  x &= 0x55;
+  x = (x | (x >> 1)) & 0x33;
+  x = (x | (x >> 2)) & 0x0f;
+  return x;
+}
+
+// Inclusive prefix of `v` over the block's threads in thread order; `total` = block sum.
+__device__ __forceinline__ uint32_t block_inclusive_sum(uint32_t v, int* warp_tot, uint32_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int incl = v;
+  uint32_t incl = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t;
   }
-  if (lane == 31) warp_tot[warp] = incl;
+  if (lane == 31) warp_tot[warp] = (int)incl;
   __syncthreads();
-  int before = 0, all = 0;
+  uint32_t before = 0, all = 0;
 #pragma unroll
   for (int w = 0; w < kWarps; ++w) {
-    const int t = warp_tot[w];
-    before += (w < warp) ? t : 0;
+    const uint32_t t = (uint32_t)warp_tot[w];
+    before += (w < warp) ? t : 0u;
     all += t;
   }
   __syncthreads();
   *total = all;
-  return before + incl - v;
+  return before + incl;
 }
 
-__global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
-    haar_topk_kernel(const float* __restrict__ faces, int S, int K, int32_t* __restrict__ idx_out,
-                     float* __restrict__ st_out, uint32_t* err) {
+// One level of the transform over LL values held in Morton order by the lanes of a warp:
+// the 2x2 block of LL grid positions (2i..2i+1, 2j..2j+1) is held by lanes
+// base, base + s, base + 2s, base + 3s (a = (2i,2j), b = (2i,2j+1), c = (2i+1,2j),
+// d = (2i+1,2j+1)).  The leader lane (base) keeps LL; the three details go to `upper` at
+// (i, j+h), (i+h, j), (i+h, j+h) of the G x G upper block, h = the new LL side.
+__device__ __forceinline__ void shuffle_level(float ll[3], int lane, int s, int m, int h, bool live,
+                                              float* upper, int G) {
+  float v[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    v[0][c] = __shfl_down_sync(0xffffffffu, ll[c], s);
+    v[1][c] = __shfl_down_sync(0xffffffffu, ll[c], 2 * s);
+    v[2][c] = __shfl_down_sync(0xffffffffu, ll[c], 3 * s);
+  }
+  if (live && (lane & (4 * s - 1)) == 0) {
+    const int j = morton_even(m), i = morton_even(m >> 1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float a, hl, lh, hh;
+      haar4(ll[c], v[0][c], v[1][c], v[2][c], a, hl, lh, hh);
+      ll[c] = a;
+      upper[(i * G + j + h) * 3 + c] = hl;
+      upper[((i + h) * G + j) * 3 + c] = lh;
+      upper[((i + h) * G + j + h) * 3 + c] = hh;
+    }
+  }
+}
+
+template <int S>
+__global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
+    haar_topk_kernel(const float* __restrict__ faces, int K, int32_t* __restrict__ idx_out,
+                     float* __restrict__ st_out) {
+  constexpr int B = S < 4 ? S : 4;   // texel block per thread: B x B
+  constexpr int G = S / B;           // thread blocks per face side; the upper block is G x G
+  constexpr int T = G * G;           // threads holding coefficients
+  constexpr int SS = S * S;
+  constexpr int NR = B == 4 ? 15 : (B == 2 ? 3 : 0);  // coefficients held in registers
+  constexpr int NW = (SS + 31) / 32;
+  static_assert(T <= kThreads, "one 4x4 block per thread");
+
   extern __shared__ __align__(16) char smem_raw[];
   HaarSmem sm;
   smem_layout(S, K, smem_raw, &sm);
   cg::cluster_group cluster = cg::this_cluster();
   const int face = (int)cluster.block_rank();
   const int env = blockIdx.x / 6;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int warp = tid >> 5, lane = tid & 31;
-  const int SS = S * S;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const float* src = faces + ((size_t)env * 6 + face) * (size_t)SS * 3;
+  const bool owner = tid < T;
+  const int bj = morton_even(tid), bi = morton_even(tid >> 1);
 
-  // ---- the face into shared memory: one bulk copy when the source allows it
-  const uint32_t face_bytes = (uint32_t)SS * 12u;
-  const bool bulk = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (face_bytes % 16 == 0);
-  if (bulk) {
-    if (tid == 0) {
-      mbar_init(sm.bar, 1);
-      fence_barrier_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-      mbar_arrive_expect_tx(sm.bar, face_bytes);
-      bulk_g2s(sm.C, src, face_bytes, sm.bar);
-    }
-    // on a timeout the face reads as whatever is in shared memory; the error is reported
-    // and every CTA still reaches the cluster barriers below
-    mbar_wait(sm.bar, 0, err);
-  } else {
-    for (int e = tid; e < SS * 3; e += nt) sm.C[e] = __ldg(src + e);
-    __syncthreads();
-  }
-  // ---- Haar levels n = S, S/2, ..., 2 in place on the top-left n x n block: each thread
-  // reads its 2x2 blocks (3 channels, two 8-byte-aligned runs of 6 floats), then after a
-  // barrier writes their LL, HL, LH, HH
-  for (int n = S, lg = 0; n >= 2; n >>= 1) {
-    const int h = n >> 1;
-    while ((1 << lg) < h) ++lg;
-    while ((1 << lg) > h) --lg;
-    float in[kMaxLevelQuads][12];
+  if (face == 0 && tid == 0) sm.scal[kScCounter] = 0;  // winner slots (read after 5 cluster barriers)
+  for (int w = tid; w < NW; w += kThreads) sm.bits[w] = 0u;
+
+  // ---- levels 1 and 2 on this thread's B x B block, in registers
+  float co[NR > 0 ? NR : 1][3];  // detail coefficients held in registers (RGB)
 #pragma unroll
-    for (int u = 0; u < kMaxLevelQuads; ++u) {
-      const int b = tid + u * nt;
-      if (b < h * h) {
-        const int i = b >> lg, j = b & (h - 1);
-        const float2* r0 = reinterpret_cast<const float2*>(sm.C + ((2 * i) * S + 2 * j) * 3);
-        const float2* r1 = reinterpret_cast<const float2*>(sm.C + ((2 * i + 1) * S + 2 * j) * 3);
+  for (int u = 0; u < (NR > 0 ? NR : 1); ++u) co[u][0] = co[u][1] = co[u][2] = 0.f;
+  float ll[3] = {0.f, 0.f, 0.f};
+  if (owner) {
+    float px[B][B][3];
+    const float* blk = src + ((size_t)(B * bi) * S + B * bj) * 3;
+    if constexpr (B == 4) {
+      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const float2 x = r0[q], y = r1[q];
-          in[u][2 * q] = x.x;
-          in[u][2 * q + 1] = x.y;
-          in[u][6 + 2 * q] = y.x;
-          in[u][6 + 2 * q + 1] = y.y;
+        for (int r = 0; r < 4; ++r) {
+          const float4* row = reinterpret_cast<const float4*>(blk + (size_t)r * S * 3);
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const float4 v = __ldg(row + q);
+            const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) px[r][(4 * q + k) / 3][(4 * q + k) % 3] = e[k];
+          }
         }
-      }
-    }
-    __syncthreads();
+      } else {
 #pragma unroll
-    for (int u = 0; u < kMaxLevelQuads; ++u) {
-      const int b = tid + u * nt;
-      if (b < h * h) {
-        const int i = b >> lg, j = b & (h - 1);
-        // in[]: row 2i = (px 2j: r g b, px 2j+1: r g b), then row 2i+1 likewise
+        for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          float ll, hl, lh, hh;
-          haar4(in[u][c], in[u][3 + c], in[u][6 + c], in[u][9 + c], ll, hl, lh, hh);
-          sm.C[(i * S + j) * 3 + c] = ll;
-          sm.C[(i * S + j + h) * 3 + c] = hl;
-          sm.C[((i + h) * S + j) * 3 + c] = lh;
-          sm.C[((i + h) * S + j + h) * 3 + c] = hh;
-        }
+          for (int q = 0; q < 12; ++q) px[r][q / 3][q % 3] = __ldg(blk + (size_t)r * S * 3 + q);
       }
+      float l1[2][2][3];
+#pragma unroll
+      for (int qi = 0; qi < 2; ++qi)
+#pragma unroll
+        for (int qj = 0; qj < 2; ++qj)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float a, hl, lh, hh;
+            haar4(px[2 * qi][2 * qj][c], px[2 * qi][2 * qj + 1][c], px[2 * qi + 1][2 * qj][c],
+                  px[2 * qi + 1][2 * qj + 1][c], a, hl, lh, hh);
+            l1[qi][qj][c] = a;
+            const int u = (qi * 2 + qj) * 3;
+            co[u][c] = hl;
+            co[u + 1][c] = lh;
+            co[u + 2][c] = hh;
+          }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float a, hl, lh, hh;
+        haar4(l1[0][0][c], l1[0][1][c], l1[1][0][c], l1[1][1][c], a, hl, lh, hh);
+        ll[c] = a;
+        co[12][c] = hl;
+        co[13][c] = lh;
+        co[14][c] = hh;
+      }
+    } else if constexpr (B == 2) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) px[r][q / 3][q % 3] = __ldg(blk + (size_t)r * S * 3 + q);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float a, hl, lh, hh;
+        haar4(px[0][0][c], px[0][1][c], px[1][0][c], px[1][1][c], a, hl, lh, hh);
+        ll[c] = a;
+        co[0][c] = hl;
+        co[1][c] = lh;
+        co[2][c] = hh;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ll[c] = __ldg(src + c);
     }
-    __syncthreads();
   }
-  // ---- keys
-  for (int p = tid; p < SS; p += nt) sm.keys[p] = wavelet_key_bits(sm.C[p * 3], sm.C[p * 3 + 1], sm.C[p * 3 + 2]);
+  // ---- the remaining levels over the G x G LL grid, held in Morton order by threads 0..T-1
+  {
+    int n = G, s = 1;  // LL grid side; lane stride between the values of one 2x2 block
+#pragma unroll
+    for (int lev = 0; lev < 2; ++lev)
+      if (n >= 2) {
+        shuffle_level(ll, lane, s, tid / (4 * s), n / 2, owner, sm.upper, G);
+        n /= 2;
+        s *= 4;
+      }
+    if (n >= 2) {
+      // at most 4 x 4 values left: leaders hand them to warp 0
+      if (owner && (tid & (s - 1)) == 0)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sm.llg[(tid / s) * 3 + c] = ll[c];
+      __syncthreads();
+      if (warp == 0) {
+        const bool live = lane < n * n;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ll[c] = live ? sm.llg[lane * 3 + c] : 0.f;
+        int s2 = 1;
+#pragma unroll
+        for (int lev = 0; lev < 2; ++lev)
+          if (n >= 2) {
+            shuffle_level(ll, lane, s2, lane / (4 * s2), n / 2, live, sm.upper, G);
+            n /= 2;
+            s2 *= 4;
+          }
+        if (lane == 0)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) sm.upper[c] = ll[c];
+      }
+    } else if (tid == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sm.upper[c] = ll[c];
+    }
+  }
+  __syncthreads();
+  // ---- this thread's 16 coefficients: NR in registers, one of the upper block
+  constexpr int NK = NR + 1;
+  // index within the face of this thread's coefficient u (u == NR: its upper-block entry)
+  auto flat_of = [&](int u) -> int {
+    if (u == NR) return (tid / G) * S + (tid % G);
+    int i = 0, j = 0, h = 1;
+    if constexpr (B == 4) {
+      const int q = u / 3;
+      i = q < 4 ? 2 * bi + (q >> 1) : bi;
+      j = q < 4 ? 2 * bj + (q & 1) : bj;
+      h = q < 4 ? S / 2 : S / 4;
+    }
+    const int band = u % 3;
+    return band == 0 ? i * S + j + h : (band == 1 ? (i + h) * S + j : (i + h) * S + j + h);
+  };
+  uint32_t key[NK];
+#pragma unroll
+  for (int u = 0; u < NR; ++u) key[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
+  float ur = 0.f, ug = 0.f, ub = 0.f;
+  if (owner) {
+    ur = sm.upper[tid * 3];
+    ug = sm.upper[tid * 3 + 1];
+    ub = sm.upper[tid * 3 + 2];
+  }
+  key[NR] = wavelet_key_bits(ur, ug, ub);
+
   // ---- 4-pass radix select of the K-th largest key over the whole cluster
   uint32_t prefix = 0, mask = 0;
   int remaining = K;
-  int* gt = sm.scal + 8;   // [6] keys above the threshold, per face
-  int* eq = sm.scal + 16;  // [6] keys equal to the threshold, per face
-  if (tid < 6) { gt[tid] = 0; eq[tid] = 0; }
   for (int pass = 0; pass < 4; ++pass) {
     const int shift = 24 - 8 * pass;
     uint32_t* h = sm.hist + (pass & 1) * 256;
     // buffer (pass & 1) was last read remotely in pass - 2, before the previous cluster barrier
-    for (int d = tid; d < 256; d += nt) h[d] = 0;
+    h[tid] = 0u;
     __syncthreads();
-    for (int p = tid; p < SS; p += nt) {
-      const uint32_t k = sm.keys[p];
-      if ((k & mask) == prefix) atomicAdd(&h[(k >> shift) & 255u], 1u);
-    }
+    if (owner)
+#pragma unroll
+      for (int u = 0; u < NK; ++u)
+        if ((key[u] & mask) == prefix) atomicAdd(&h[(key[u] >> shift) & 255u], 1u);
     cluster.sync();
-    if (tid < 256) {
-      uint32_t v[6];
+    const int digit = 255 - tid;  // thread order = digits from the top
+    uint32_t v[6], tot = 0;
 #pragma unroll
-      for (int g = 0; g < 6; ++g) v[g] = cluster.map_shared_rank(h, g)[tid];
-      uint32_t t = 0;
+    for (int g = 0; g < 6; ++g) v[g] = cluster.map_shared_rank(h, g)[digit];
 #pragma unroll
-      for (int g = 0; g < 6; ++g) {
-        sm.all_h[g * 256 + tid] = v[g];
-        t += v[g];
-      }
-      sm.tot[tid] = t;
+    for (int g = 0; g < 6; ++g) tot += v[g];
+    uint32_t all;
+    const uint32_t incl = block_inclusive_sum(tot, sm.warp_tot, &all);
+    if (incl >= (uint32_t)remaining && incl - tot < (uint32_t)remaining) {
+      sm.scal[kScPrefix] = (int)(prefix | ((uint32_t)digit << shift));
+      sm.scal[kScMask] = (int)(mask | (255u << shift));
+      sm.scal[kScRemaining] = remaining - (int)(incl - tot);
+      if (pass == 3)
+#pragma unroll
+        for (int g = 0; g < 6; ++g) sm.scal[kScEq + g] = (int)v[g];
     }
     __syncthreads();
-    if (warp == 0) {
-      // lane l covers digits 255-8l .. 248-8l (highest digits first)
-      const int d_hi = 255 - 8 * lane;
-      uint32_t tot8[8];
-      uint32_t local = 0;
+    prefix = (uint32_t)sm.scal[kScPrefix];
+    mask = (uint32_t)sm.scal[kScMask];
+    remaining = sm.scal[kScRemaining];
+  }
+  // ---- ties at the threshold, taken in flat-index order (faces in order)
+  const uint32_t thr = prefix;
+  int eq_before = 0;
+  for (int g = 0; g < face; ++g) eq_before += sm.scal[kScEq + g];
+  if (owner)
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        tot8[q] = sm.tot[d_hi - q];
-        local += tot8[q];
+    for (int u = 0; u < NK; ++u)
+      if (key[u] == thr) {
+        const int f = flat_of(u);
+        atomicOr(&sm.bits[f >> 5], 1u << (f & 31));
       }
-      uint32_t incl = local;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const uint32_t excl = incl - local;
-      const unsigned hit = __ballot_sync(0xffffffffu, incl >= (uint32_t)remaining);
-      const int cl = __ffs(hit) - 1;  // the total count >= remaining, so hit != 0
-      int dsel = 0;
-      uint32_t above = 0;
-      if (lane == cl) {
-        uint32_t cum = excl;
-        for (int q = 0; q < 8; ++q) {
-          if (cum + tot8[q] >= (uint32_t)remaining) { dsel = d_hi - q; break; }
-          cum += tot8[q];
-        }
-        above = cum;
-      }
-      dsel = __shfl_sync(0xffffffffu, dsel, cl);
-      above = __shfl_sync(0xffffffffu, above, cl);
-      if (lane == 0) {
-        sm.scal[0] = (int)(prefix | ((uint32_t)dsel << shift));
-        sm.scal[1] = (int)(mask | (255u << shift));
-        sm.scal[2] = remaining - (int)above;
-        sm.scal[3] = dsel;
-      }
-    }
-    __syncthreads();
-    prefix = (uint32_t)sm.scal[0];
-    mask = (uint32_t)sm.scal[1];
-    remaining = sm.scal[2];
-    // per-face counts of keys whose digit is above the selected one (warp g: face g)
-    if (warp < 6) {
-      const int dsel = sm.scal[3];
-      const int d_hi = 255 - 8 * lane;
-      uint32_t s = 0;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int d = d_hi - q;
-        s += d > dsel ? sm.all_h[warp * 256 + d] : 0u;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) {
-        gt[warp] += (int)s;
-        if (pass == 3) eq[warp] = (int)sm.all_h[warp * 256 + dsel];
-      }
-    }
-    // the next pass starts with a barrier; the loop's last one follows below
+  __syncthreads();
+  {
+    uint32_t all;
+    const uint32_t c = tid < NW ? (uint32_t)__popc(sm.bits[tid]) : 0u;
+    const uint32_t incl = block_inclusive_sum(c, sm.warp_tot, &all);
+    if (tid < NW) sm.wpre[tid] = incl - c;
   }
   __syncthreads();
-  // ---- this face's share of the winners
-  const uint32_t thr = prefix;
-  int eq_before = 0, n_before = 0;
-  for (int g = 0; g < face; ++g) {
-    int take_g = remaining - eq_before;
-    take_g = take_g < 0 ? 0 : (take_g > eq[g] ? eq[g] : take_g);
-    n_before += gt[g] + take_g;
-    eq_before += eq[g];
-  }
-  int take = remaining - eq_before;
-  take = take < 0 ? 0 : (take > eq[face] ? eq[face] : take);
-  uint64_t* dkey = cluster.map_shared_rank(sm.gkey, 0);
-  Gathered* dval = cluster.map_shared_rank(sm.gval, 0);
-  // thread t owns keys [t*per, t*per + per): ties get their flat-index rank from one
-  // ordered scan; the winners' slots in CTA 0 only need to be distinct (the final rank
-  // orders them), so they come from a shared counter
-  const int per = (SS + nt - 1) / nt;
-  const int p0 = tid * per;
-  int n_tie_mine = 0;
+  // ---- winners: slots from CTA 0's counter (one atomic per warp), stored in every CTA
+  uint32_t selmask = 0;
+  int n_sel = 0;
+  if (owner)
 #pragma unroll
-  for (int u = 0; u < kMaxPerThread; ++u) {
-    const int p = p0 + u;
-    if (u < per && p < SS && sm.keys[p] == thr) ++n_tie_mine;
-  }
-  int *counter = sm.scal + 24;
-  if (tid == 0) *counter = 0;
-  int n_tie_all;
-  int tie_rank = block_exclusive_sum(n_tie_mine, sm.warp_tot, &n_tie_all);
-#pragma unroll
-  for (int u = 0; u < kMaxPerThread; ++u) {
-    const int p = p0 + u;
-    if (u >= per || p >= SS) continue;
-    const uint32_t k = sm.keys[p];
-    bool sel = k > thr;
-    if (k == thr) sel = tie_rank++ < take;
-    if (sel) {
-      const int slot = n_before + atomicAdd(counter, 1);
-      const int32_t flat = face * SS + p;
-      // composite key: larger key first, then smaller index first
-      dkey[slot] = ((uint64_t)k << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)flat);
-      dval[slot] = Gathered{sm.C[p * 3], sm.C[p * 3 + 1], sm.C[p * 3 + 2], flat};
+    for (int u = 0; u < NK; ++u) {
+      bool sel = key[u] > thr;
+      if (key[u] == thr) {
+        const int f = flat_of(u), w = f >> 5;
+        const int rank = eq_before + (int)sm.wpre[w] + __popc(sm.bits[w] & ((1u << (f & 31)) - 1u));
+        sel = rank < remaining;
+      }
+      if (sel) {
+        selmask |= 1u << u;
+        ++n_sel;
+      }
     }
+  int incl_w = n_sel;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl_w, o);
+    if (lane >= o) incl_w += t;
+  }
+  int base = 0;
+  if (lane == 31 && incl_w > 0) base = atomicAdd(cluster.map_shared_rank(&sm.scal[kScCounter], 0), incl_w);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  int slot = base + incl_w - n_sel;
+  if (selmask) {
+#pragma unroll
+    for (int u = 0; u < NK; ++u)
+      if (selmask & (1u << u)) {
+        const int32_t gflat = face * SS + flat_of(u);
+        // composite key: larger key first, then smaller index first
+        const uint64_t ck = ((uint64_t)key[u] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)gflat);
+        Winner wv;
+        if (u < NR) {
+          wv = Winner{co[u][0], co[u][1], co[u][2], gflat};
+        } else {
+          wv = Winner{ur, ug, ub, gflat};
+        }
+#pragma unroll
+        for (int g = 0; g < 6; ++g) {
+          cluster.map_shared_rank(sm.gkey, g)[slot] = ck;
+          cluster.map_shared_rank(sm.gval, g)[slot] = wv;
+        }
+        ++slot;
+      }
   }
   cluster.sync();
-  // ---- rank the K winners (CTA 0)
-  if (face == 0) {
-    for (int e = tid; e < K; e += nt) {
-      const uint64_t me = sm.gkey[e];
-      int rank = 0;
-      for (int o = 0; o < K; ++o) rank += sm.gkey[o] > me;
-      const Gathered v = sm.gval[e];
+  // ---- rank the K winners: CTA f takes winners f, f + 6, ...; one warp per winner
+  for (int e = face + 6 * warp; e < K; e += 6 * kWarps) {
+    const uint64_t me = sm.gkey[e];
+    int rank = 0;
+    for (int o = lane; o < K; o += 32) rank += sm.gkey[o] > me;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rank += __shfl_xor_sync(0xffffffffu, rank, o);
+    if (lane == 0) {
+      const Winner wv = sm.gval[e];
       const size_t out = (size_t)env * K + rank;
-      idx_out[out] = v.idx;
-      st_out[out * 3 + 0] = v.r;
-      st_out[out * 3 + 1] = v.g;
-      st_out[out * 3 + 2] = v.b;
+      idx_out[out] = wv.idx;
+      st_out[out * 3 + 0] = wv.r;
+      st_out[out * 3 + 1] = wv.g;
+      st_out[out * 3 + 2] = wv.b;
     }
   }
+}
+
+template <int S>
+void launch_s(const float* faces, int n_env, int K, int32_t* idx, float* strength, cudaStream_t st) {
+  const size_t smem = smem_layout(S, K, nullptr, nullptr);
+  NWPRT_CUDA(cudaFuncSetAttribute(haar_topk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  haar_topk_kernel<S><<<6 * n_env, kThreads, smem, st>>>(faces, K, idx, strength);
+  NWPRT_CUDA(cudaGetLastError());
 }
 
 }  // namespace
@@ -362,7 +466,7 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads)
 size_t haar_topk_smem_bytes(int S, int K) { return smem_layout(S, K, nullptr, nullptr); }
 
 void launch_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx, float* strength,
-                      uint32_t* err, cudaStream_t st) {
+                      uint32_t* /*err: the kernel has no waits that could time out*/, cudaStream_t st) {
   if (n_env < 1 || n_env > (1 << 28)) fail(NWPRT_INVALID_ARG, "haar_topk: n_env out of range");
   if (S < 1 || S > kMaxS || (S & (S - 1)))
     fail(S > kMaxS ? NWPRT_UNSUPPORTED : NWPRT_INVALID_ARG,
@@ -370,10 +474,15 @@ void launch_haar_topk(const float* faces, int n_env, int S, int K, int32_t* idx,
   if (K < 1 || K > 6 * S * S || K > kMaxK)
     fail(NWPRT_INVALID_ARG, "haar_topk: K must be in [1, min(6*S*S, 1024)]");
   if (!faces || !idx || !strength) fail(NWPRT_INVALID_ARG, "haar_topk: null pointer");
-  const size_t smem = haar_topk_smem_bytes(S, K);
-  NWPRT_CUDA(cudaFuncSetAttribute(haar_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  haar_topk_kernel<<<6 * n_env, kThreads, smem, st>>>(faces, S, K, idx, strength, err);
-  NWPRT_CUDA(cudaGetLastError());
+  switch (S) {
+    case 1: launch_s<1>(faces, n_env, K, idx, strength, st); break;
+    case 2: launch_s<2>(faces, n_env, K, idx, strength, st); break;
+    case 4: launch_s<4>(faces, n_env, K, idx, strength, st); break;
+    case 8: launch_s<8>(faces, n_env, K, idx, strength, st); break;
+    case 16: launch_s<16>(faces, n_env, K, idx, strength, st); break;
+    case 32: launch_s<32>(faces, n_env, K, idx, strength, st); break;
+    default: launch_s<64>(faces, n_env, K, idx, strength, st); break;
+  }
 }
 
 }  // namespace nwprt

@@ -182,6 +182,9 @@ bool relight_tc_supported(const NetDims& d, std::string* why);
 void launch_wait_selftest(int timeout_ms, uint32_t* err, cudaStream_t st);
 bool relight_tc_fp8_supported(const NetDims& d, std::string* why);
 size_t tc_weight_bytes(const NetDims& d);
+// Device allocation for a tensor-core weight blob of `bytes`: whole 256-byte rows, the
+// 2-D view through which the relight kernel loads it with TMA (the padding is zero).
+inline size_t tc_blob_alloc_bytes(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 // BF16 weight blob; returns its plan (with V_last), which every BF16 launch needs.
 TcPlan pack_tc_weights(const NetDims& d, const float* op, const float* cn, std::vector<uint16_t>* out);
 // FP8 weight blob from calibrated activation maxima amax[0..n_layers) (the input of every

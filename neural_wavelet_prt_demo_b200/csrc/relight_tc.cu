@@ -34,6 +34,8 @@
 // generic form that reads the sequence from the plan.  Every wait is bounded by
 // %globaltimer (2 s); on expiry the kernel records kDevWaitTimeout and the warpgroup
 // unwinds together.
+#include <cuda.h>  // CUtensorMap; cuTensorMapEncodeTiled is resolved through the runtime
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -59,11 +61,18 @@ constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kInlineJobs = 256;
 static_assert(kNWG * kTileCols <= kTmemCols, "TMEM budget");
 
+// The weight blob is loaded with TMA through a 2-D view: rows of kWRowBytes bytes, in
+// w_boxes boxes of w_box_rows rows (the last box may extend past the blob; its rows read as
+// zeros and land inside the shared-memory weight region, which holds whole boxes).
+constexpr uint32_t kWRowBytes = 256;
+constexpr uint32_t kWMaxBoxRows = 256;
+
 struct TcParams {
+  CUtensorMap wmap;  // the weight blob, [rows][kWRowBytes / 4] uint32
   HashLevels hl;
   const float* hash;
-  const uint4* wblob;
   uint32_t wblob_bytes;
+  uint32_t w_boxes, w_box_rows;
   TcLayer layers[kMaxTcLayers];
   int n_layers;
   int enc_dims;  // D, multiple of 16, <= 32
@@ -462,8 +471,22 @@ __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long
 struct __align__(8) TcBarriers {
   uint64_t acc_full[kNWG];  // MMA commit -> epilogue of that warpgroup's tile
   uint64_t done[kNWG];      // final commit before TMEM is released
+  uint64_t wload;           // the weight blob's TMA load
   uint32_t tmem_base;
 };
+
+// Shared-memory bytes of the weight region: whole TMA boxes, rounded to 1 KB.
+__host__ __device__ inline uint32_t weight_region_bytes(uint32_t boxes, uint32_t box_rows) {
+  return (boxes * box_rows * kWRowBytes + 1023u) & ~1023u;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
 
 // Layer sequences fixed at compile time, so that the per-layer flags are constants and the
 // layer loop unrolls (the plan still supplies offsets, strides and scales).  kShapePlan: the
@@ -520,8 +543,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   using Sh = ShapeOf<SHAPE>;
   const int n_layers = SHAPE ? Sh::nl : p.n_layers;
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* wsm = smem;                                       // weight blob
-  uint8_t* aux = smem + ((p.wblob_bytes + 1023u) & ~1023u);  // [kNWG][kAuxBytes]
+  uint8_t* wsm = smem;                                                  // weight blob
+  uint8_t* aux = smem + weight_region_bytes(p.w_boxes, p.w_box_rows);  // [kNWG][kAuxBytes]
   uint32_t* encs = reinterpret_cast<uint32_t*>(aux + kNWG * kAuxBytes);  // [kNWG][DMAX/2][kTile]
   TcBarriers* bars = reinterpret_cast<TcBarriers*>(encs + kNWG * (DMAX / 2) * kTile);
   const int tid = threadIdx.x;
@@ -530,15 +553,17 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   const int q = warp & 3;   // TMEM lane quarter this warp may access
   const int row = q * 32 + lane;
 
-  // ---- weights -> shared memory (generic proxy), barriers, TMEM
-  for (uint32_t i = tid; i < p.wblob_bytes / 16u; i += kThreads)
-    reinterpret_cast<uint4*>(wsm)[i] = __ldg(p.wblob + i);
+  // ---- barriers, then the weights -> shared memory by TMA (one load per box), and TMEM
   if (tid == 0) {
     for (int w = 0; w < kNWG; ++w) {
       mbar_init(&bars->acc_full[w], 1);
       mbar_init(&bars->done[w], 1);
     }
+    mbar_init(&bars->wload, 1);
     fence_barrier_init();
+    mbar_arrive_expect_tx(&bars->wload, p.w_boxes * p.w_box_rows * kWRowBytes);
+    for (uint32_t b = 0; b < p.w_boxes; ++b)
+      tma_load_2d(wsm + b * p.w_box_rows * kWRowBytes, &p.wmap, 0, (int)(b * p.w_box_rows), &bars->wload);
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -547,10 +572,11 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  fence_proxy_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  // the weights have landed (every thread sees the barrier complete before any MMA reads them)
+  bool ok = wait_bounded(&bars->wload, 0, p.err);
   const uint32_t tmem = bars->tmem_base;
   const uint32_t wbase = smem_u32(wsm);
   const long long stride = (long long)gridDim.x * kNWG;
@@ -564,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   uint64_t* acc_bar = &bars->acc_full[g];
 
   uint32_t ph = 0;
-  bool ok = true;
+  ok = wg_barrier_and(g, ok);
   for (long long t = (long long)blockIdx.x * kNWG + g; t < p.total_tiles && ok; t += stride) {
     // ---- tile set-up: hash encoding, aux operand, first-layer operand of wavelet 0
     const int jid = find_job(p.jobs, p.n_jobs, t);
@@ -990,9 +1016,55 @@ int shape_of(const TcPlan& P, const NetDims& d) {
 
 size_t enc_smem_bytes(const NetDims& d) { return (size_t)kNWG * (d.enc_dims() <= 16 ? 8 : 16) * kTile * 4; }
 
-size_t relight_tc_smem_bytes(const NetDims& d) {
-  return ((tc_weight_bytes(d) + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + enc_smem_bytes(d) +
-         sizeof(TcBarriers);
+// Rows of the weight blob's TMA view and their split into boxes of at most kWMaxBoxRows rows.
+void weight_boxes(uint32_t blob_bytes, uint32_t* rows, uint32_t* boxes, uint32_t* box_rows) {
+  *rows = (blob_bytes + kWRowBytes - 1) / kWRowBytes;
+  *boxes = (*rows + kWMaxBoxRows - 1) / kWMaxBoxRows;
+  *box_rows = (*rows + *boxes - 1) / *boxes;
+}
+
+size_t smem_for_blob(const NetDims& d, uint32_t blob_bytes) {
+  uint32_t rows, boxes, box_rows;
+  weight_boxes(blob_bytes, &rows, &boxes, &box_rows);
+  return weight_region_bytes(boxes, box_rows) + (size_t)kNWG * kAuxBytes + enc_smem_bytes(d) + sizeof(TcBarriers);
+}
+
+size_t relight_tc_smem_bytes(const NetDims& d) { return smem_for_blob(d, (uint32_t)tc_weight_bytes(d)); }
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime.
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  if (!fn) fail(NWPRT_CUDA_ERROR, "cuTensorMapEncodeTiled is unavailable from the driver");
+  return fn;
+}
+
+// The weight blob (a device allocation of tc_blob_alloc_bytes(blob_bytes): whole rows) as a
+// [rows][kWRowBytes / 4] uint32 tensor; no swizzle, so shared memory receives the blob's
+// byte layout unchanged.
+void encode_weight_map(CUtensorMap* map, const void* blob_dev, uint32_t blob_bytes, uint32_t* boxes,
+                       uint32_t* box_rows) {
+  uint32_t rows;
+  weight_boxes(blob_bytes, &rows, boxes, box_rows);
+  if ((reinterpret_cast<uintptr_t>(blob_dev) & 15) != 0) fail(NWPRT_INVALID_ARG, "weight blob not 16-byte aligned");
+  const cuuint64_t dims[2] = {kWRowBytes / 4, rows};
+  const cuuint64_t strides[1] = {kWRowBytes};
+  const cuuint32_t box[2] = {kWRowBytes / 4, *box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(blob_dev), dims, strides,
+                                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(NWPRT_CUDA_ERROR, "cuTensorMapEncodeTiled failed for the weight blob");
 }
 
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
@@ -1014,8 +1086,8 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   TcParams p{};
   p.hl = hl;
   p.hash = hash;
-  p.wblob = reinterpret_cast<const uint4*>(blob_dev);
   p.wblob_bytes = P.blob_bytes;
+  encode_weight_map(&p.wmap, blob_dev, P.blob_bytes, &p.w_boxes, &p.w_box_rows);
   std::memcpy(p.vlast, P.vlast, sizeof(p.vlast));
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
   p.n_layers = P.n_layers;
@@ -1039,8 +1111,7 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   NWPRT_CUDA(cudaGetDevice(&dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   NWPRT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const size_t smem = ((P.blob_bytes + 1023) & ~size_t(1023)) + (size_t)kNWG * kAuxBytes + enc_smem_bytes(d) +
-                      sizeof(TcBarriers);
+  const size_t smem = smem_for_blob(d, P.blob_bytes);
   if (smem > (size_t)max_smem) fail(NWPRT_UNSUPPORTED, "tensor-core relight: shared memory budget exceeded");
   const long long groups = (tiles + kNWG - 1) / kNWG;
   const int grid = (int)(groups < sms ? groups : sms);

@@ -54,6 +54,12 @@ class Request:
     faces: Optional[np.ndarray] = None   # [6,S,S,3] for "new"
     base_env: int = -1                   # resident env index for "rot"
     R: Optional[np.ndarray] = None       # 3x3 rotation for "rot"
+    # a row band of the frame: pixels [px_lo, px_hi) (px_hi <= 0: to the end of the frame);
+    # multi-GPU serving splits large requests into one band per rank (dispatch.py)
+    px_lo: int = 0
+    px_hi: int = 0
+    owner: int = 0            # rank that reports the request (and gathers its bands)
+    split: bool = False       # one band of a request split across ranks
     # filled by the server (max_queue_s: longest a request may wait for admission)
     n_px: int = 0
     next_px: int = 0
@@ -187,6 +193,39 @@ def make_stream(n: int, rate: float, seed: int = 0, face_size: int = 64, p_new: 
 
 # ---------------------------------------------------------------------------- GPU server
 
+class LocalCompletion:
+    """What happens when a request's last quantum has run: on one GPU, it is done.  The
+    multi-GPU dispatcher (dispatch.BandGather) replaces it so that bands of split requests
+    are gathered before the request counts as done."""
+
+    def admitted(self, r: "Request") -> None:
+        pass
+
+    def finished(self, r: "Request") -> bool:
+        """The request's local work has run; True if it is complete now."""
+        return True
+
+    def failed(self, r: "Request") -> None:
+        """The request ended without its local work (refused, timed out or failed)."""
+
+    def poll(self) -> List["Request"]:
+        """Requests that completed since the last call through events outside this server."""
+        return []
+
+    def outstanding(self) -> bool:
+        return False
+
+
+class _HostEvent:
+    """Stand-in for a CUDA event when the server drives a CPU engine (tests)."""
+
+    def record(self, stream=None):
+        pass
+
+    def synchronize(self):
+        pass
+
+
 class RelightServer:
     """Serves a list of requests in real time on one GPU through one RenderEngine."""
 
@@ -194,7 +233,7 @@ class RelightServer:
                  quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
                  max_in_flight: int = 2, keep_outputs: bool = False,
                  fault: Optional[Callable[[Request, str], Optional[str]]] = None,
-                 max_active: Optional[int] = None, order: str = "fifo"):
+                 max_active: Optional[int] = None, order: str = "fifo", completion=None):
         import torch
         self.torch = torch
         self.e = engine
@@ -211,7 +250,9 @@ class RelightServer:
         self.order = order  # quantum packing order: "srpt" (least remaining work) or "fifo"
         self.keep_outputs = keep_outputs
         self.fault = fault
-        self.stream = torch.cuda.current_stream()
+        self.completion = completion or LocalCompletion()
+        self.on_gpu = frames[0].fbPredictedIndirect.is_cuda
+        self.stream = torch.cuda.current_stream() if self.on_gpu else None
         info = engine.networkInfo()
         self.face_size, self.enc_dims = info.face_size, info.enc_dims
         self.quanta = 0
@@ -236,6 +277,7 @@ class RelightServer:
     def _end_failed(self, r: Request, t: float) -> None:
         """Ends a request that failed after admission: returns its budget and env table."""
         r.status, r.t_done = "error", t
+        self.completion.failed(r)
         if r.bytes_held:
             self.adm.give(r.bytes_held)
             r.bytes_held = 0
@@ -262,27 +304,48 @@ class RelightServer:
                     failed.append(r)
             return failed
 
-    def run(self, requests: List[Request], realtime: bool = True) -> Dict:
+    def _retire(self, r: Request, t: float) -> None:
+        """A request whose work (and gather) is complete: returns its budget and env table."""
+        r.status, r.t_done = "done", t
+        self.adm.give(r.bytes_held)
+        r.bytes_held = 0
+        self.e.releaseEnvironmentMap(r.env_id)
+        r.env_id = -1
+        if not self.keep_outputs:
+            r.outputs = ()
+
+    def _refuse(self, r: Request, status: str, t: float) -> None:
+        r.status, r.t_done = status, t
+        self.completion.failed(r)
+
+    def run(self, requests: List[Request], realtime: bool = True, t0: Optional[float] = None) -> Dict:
+        """Serves `requests` (arrival times in seconds after t0, default: now)."""
         torch = self.torch
         pending: Deque[Request] = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
         queue: Deque[Request] = deque()
         active: List[Request] = []
+        gathering: List[Request] = []
         in_flight: Deque[Tuple] = deque()
         for r in requests:
             ok = isinstance(r.res, (int, np.integer)) and 0 <= r.res < len(self.frames)
-            r.n_px = self.frames[r.res].width * self.frames[r.res].height if ok else 0
-            r.next_px = 0
+            full = self.frames[r.res].width * self.frames[r.res].height if ok else 0
+            r.n_px = min(r.px_hi, full) if r.px_hi > 0 else full
+            r.next_px = max(0, r.px_lo)
             r.status = "pending"
-        t0 = time.perf_counter()
+        t0 = time.perf_counter() if t0 is None else t0
         now = lambda: time.perf_counter() - t0
         finished = 0
         total = len(requests)
         while finished < total:
+            for r in self.completion.poll():
+                gathering.remove(r)
+                self._retire(r, now())
+                finished += 1
             t = now() if realtime else math.inf
             while pending and pending[0].arrival <= t:
                 r = pending.popleft()
                 if self.fault is not None and self.fault(r, "arrive") == "drop":
-                    r.status, r.t_done = "dropped", now()
+                    self._refuse(r, "dropped", now())
                     finished += 1
                     continue
                 r.status = "queued"
@@ -294,19 +357,19 @@ class RelightServer:
                     validate_request(r, len(self.frames), self.face_size, len(self.base_faces))
                 except ValueError:
                     queue.popleft()
-                    r.status, r.t_done = "error", now()
+                    self._refuse(r, "error", now())
                     finished += 1
                     continue
                 nbytes = request_bytes(r.n_px, r.K, self.face_size, self.enc_dims)
                 if nbytes > self.adm.budget:
                     queue.popleft()
-                    r.status, r.t_done = "rejected", now()
+                    self._refuse(r, "rejected", now())
                     finished += 1
                     continue
                 if not self.adm.fits(nbytes):
                     if realtime and now() - r.arrival > self.max_queue_s:
                         queue.popleft()
-                        r.status, r.t_done = "timeout", now()
+                        self._refuse(r, "timeout", now())
                         finished += 1
                         continue
                     break
@@ -322,6 +385,7 @@ class RelightServer:
                 self.adm.take(nbytes)
                 r.bytes_held = nbytes
                 r.status, r.t_admit = "active", now()
+                self.completion.admitted(r)
                 active.append(r)
             self.max_active = max(self.max_active, len(active))
             if active and len(in_flight) < self.max_in_flight:
@@ -349,7 +413,7 @@ class RelightServer:
                 for r, _, e in launch:
                     if r.status == "active":
                         r.next_px = e
-                ev = torch.cuda.Event()
+                ev = torch.cuda.Event() if self.on_gpu else _HostEvent()
                 ev.record(self.stream)
                 done_now = [r for r, _, _ in launch if r.status == "active" and r.next_px >= r.n_px]
                 for r in done_now:
@@ -362,18 +426,20 @@ class RelightServer:
                 ev.synchronize()
                 t = now()
                 for r in done_now:
-                    r.status, r.t_done = "done", t
-                    self.adm.give(r.bytes_held)
-                    self.e.releaseEnvironmentMap(r.env_id)
-                    if not self.keep_outputs:
-                        r.outputs = ()
-                    finished += 1
+                    if self.completion.finished(r):
+                        self._retire(r, t)
+                        finished += 1
+                    else:
+                        r.status = "gathering"
+                        gathering.append(r)
                 continue
-            if pending:
-                if realtime:
+            if pending or self.completion.outstanding():
+                if realtime and pending:
                     dt = pending[0].arrival - now()
                     if dt > 0:
                         time.sleep(min(dt, 0.002))
+                elif self.completion.outstanding():
+                    time.sleep(0.0002)
                 continue
             if queue:  # nothing active, nothing in flight, but the head does not fit: cannot happen
                 raise RuntimeError("admission stalled")

@@ -9,12 +9,14 @@ collective the bench uses (a max over ranks of the elapsed time).
   across GPUs; each rank relights its band from its own copy of the G-buffer rows).
 * ``assign_requests``-- requests to ranks, balanced by estimated cost W*H*K (longest
   processing time first, ties by request index, so every rank computes the same plan).
+* ``assign_online``  -- the same balance for a stream, decided in arrival order from the
+  estimated backlog of every rank; large requests are split into row bands across ranks.
 * ``max_over_ranks`` -- torch.distributed all-reduce MAX (NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
 import heapq
-from typing import List, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 
 def row_band(height: int, rank: int, world: int) -> Tuple[int, int]:
@@ -50,6 +52,38 @@ def assign_requests(costs: Sequence[int], world: int) -> List[List[int]]:
         heapq.heappush(heap, (load + int(costs[i]), r))
     for lst in out:
         lst.sort()
+    return out
+
+
+def assign_online(arrivals: Sequence[float], costs: Sequence[int], world: int, evals_per_s: float,
+                  split_min_evals: Optional[int] = None, heights: Optional[Sequence[int]] = None
+                  ) -> List[Tuple[int, bool]]:
+    """Placement of a request stream on ranks, decided request by request in arrival order.
+
+    Every rank keeps the same estimate of each rank's backlog (draining at `evals_per_s`),
+    so every rank computes the same plan without communicating.  A request goes to the rank
+    that would start it first (lowest rank on ties).  A request of at least
+    `split_min_evals` evaluations whose frame has at least `world` rows is split into one
+    row band per rank (``row_band``); each band adds its share to its rank's backlog, and the
+    request is owned (its bands gathered and its latency reported) by the rank that would
+    have started it first.  Returns (owner, split) per request."""
+    if world < 1 or evals_per_s <= 0:
+        raise ValueError("world must be >= 1 and evals_per_s > 0")
+    free = [0.0] * world
+    out: List[Tuple[int, bool]] = []
+    for i, (a, c) in enumerate(zip(arrivals, costs)):
+        a = float(a)
+        starts = [max(f, a) for f in free]
+        owner = min(range(world), key=lambda r: (starts[r], r))
+        h = heights[i] if heights is not None else world
+        split = world > 1 and split_min_evals is not None and int(c) >= split_min_evals and h >= world
+        if split:
+            for r in range(world):
+                b, e = row_band(h, r, world)
+                free[r] = starts[r] + int(c) * (e - b) / h / evals_per_s
+        else:
+            free[owner] = starts[owner] + int(c) / evals_per_s
+        out.append((owner, split))
     return out
 
 
