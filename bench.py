@@ -57,8 +57,11 @@ def parse_args():
                     help="serve: kernel time per scheduling quantum")
     ap.add_argument("--serve-nets", choices=["both", "large", "small"], default="both",
                     help="serve: which network(s) to run (config 2, config 0, or both)")
-    ap.add_argument("--serve-order", choices=["fifo", "srpt"], default="fifo",
-                    help="serve: quantum packing order (arrival, or least remaining work)")
+    ap.add_argument("--serve-order", choices=["fifo", "srpt", "edf"], default="fifo",
+                    help="serve: quantum packing order (arrival, least remaining work, or earliest "
+                         "deadline with deadlines proportional to request size)")
+    ap.add_argument("--serve-adaptive", action="store_true",
+                    help="serve: shrink a quantum when an admitted request has not started within one")
     ap.add_argument("--serve-max-active", type=int, default=0,
                     help="serve: admit at most this many requests at once (0: the byte budget alone)")
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
@@ -763,10 +766,17 @@ def _measure_rate(e, frames, base, precision):
 def run_serve(args, rank, world, local, dev):
     """Config-4 serving stream: Poisson arrivals, mixed resolution / K / env maps (40% new,
     60% rotations of resident maps), budget admission, continuous batching.  Reports
-    throughput and p50/p99 latency of the served BF16 path, the same for a small (config-0)
-    network, and the plain FP32 serial baseline on a prefix of the stream."""
+    throughput and p50/p99 latency (overall, and for frames up to 720p vs larger ones) of the
+    served BF16 path, the same for a small (config-0) network, and the plain FP32 serial
+    baseline on a prefix of the stream.
+
+    Every rank serves the SAME stream: with N GPUs it is split by the dispatcher (requests
+    placed by estimated backlog, frames of >= 1080p at K=300 split into row bands gathered at
+    their owner with NCCL point-to-point transfers), so N only changes how fast the fixed
+    stream is served ("strong" scaling)."""
     import torch
-    from neural_wavelet_prt_demo_b200 import netconfig, serve
+    import torch.distributed as dist
+    from neural_wavelet_prt_demo_b200 import dispatch, netconfig, serve
     out = {}
     sampler = ClockSampler(local)
     nets = [("served_bf16", netconfig.CONFIG_LARGE, 64), ("served_bf16_small_net", netconfig.CONFIG_SMALL, 32)]
@@ -774,46 +784,78 @@ def run_serve(args, rank, world, local, dev):
         nets = nets[:1]
     elif args.serve_nets == "small":
         nets = nets[1:]
+    channels = dispatch.PairChannels(world) if world > 1 else None
     clocks = None
     for name, cfg, S in nets:
         e, frames, base = _serve_rig(cfg, S, dev)
         rate = _measure_rate(e, frames, base, "bf16")
-        reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=rank, face_size=S)
-        srv = serve.RelightServer(e, frames, base, precision="bf16", budget_bytes=150 << 30,
-                                  quantum_ms=args.serve_quantum_ms, est_evals_per_s=rate,
-                                  max_active=args.serve_max_active or None, order=args.serve_order)
+        if world > 1:  # every rank plans with the same estimate
+            t = torch.tensor([rate], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+            rate = float(t.item())
+        reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=0, face_size=S)
+        kw = dict(precision="bf16", budget_bytes=150 << 30, quantum_ms=args.serve_quantum_ms, est_evals_per_s=rate,
+                  max_active=args.serve_max_active or None, order=args.serve_order,
+                  adaptive_quantum=args.serve_adaptive)
+        frame_px = [f.width * f.height for f in frames]
         first = clocks is None
         if first:
             sampler.start()
-        st = srv.run(reqs)
+        if world > 1:
+            torch.cuda.synchronize()
+            dist.barrier()
+            mine = dispatch.serve_distributed(e, frames, base, reqs, rank, world, channels, dev, rate,
+                                              server_kwargs=kw)
+            local_reqs = mine.pop("local")
+            owned = [r for r in local_reqs if r.owner == rank or not r.split]
+            mine["classes_local"] = [(frame_px[r.res], r.latency * 1e3) for r in owned if r.status == "done"]
+            all_s = [None] * world
+            dist.all_gather_object(all_s, mine)
+            st = dispatch.combine_summaries(all_s)
+            cls = {}
+            for cname, pick in (("small", lambda n: n <= serve.SMALL_CLASS_MAX_PX),
+                                ("large", lambda n: n > serve.SMALL_CLASS_MAX_PX)):
+                lat = [l for s_ in all_s for (n, l) in s_["classes_local"] if pick(n)]
+                cls[cname] = {"done": len(lat), "p50_ms": serve.percentile(lat, 50), "p99_ms": serve.percentile(lat, 99)}
+            st["classes"] = cls
+        else:
+            srv = serve.RelightServer(e, frames, base, **kw)
+            st = srv.run(reqs)
+            st.update({"quanta": srv.quanta, "max_concurrent": srv.max_active,
+                       "classes": serve.class_latency(reqs, frame_px)})
         if first:
             clocks = sampler.stop()
-        st.update({"quanta": srv.quanta, "max_concurrent": srv.max_active, "kernel_evals_per_s_1080p": rate,
-                   "offered_evals_per_s": sum(r.n_px * r.K for r in reqs) / reqs[-1].arrival})
+        st.update({"kernel_evals_per_s_1080p": rate,
+                   "offered_evals_per_s": sum(frame_px[r.res] * r.K for r in reqs) / reqs[-1].arrival})
         out[name] = st
-        if name == "served_bf16" and args.serve_serial_prefix > 0:
+        if name == "served_bf16" and args.serve_serial_prefix > 0 and world == 1:
             m = args.serve_serial_prefix
-            prefix = serve.make_stream(m, args.serve_rate, seed=rank, face_size=S)
+            prefix = serve.make_stream(m, args.serve_rate, seed=0, face_size=S)
             st2 = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=args.serve_quantum_ms,
                                       est_evals_per_s=rate).run(prefix)
             out["served_bf16_prefix"] = st2
-            prefix = serve.make_stream(m, args.serve_rate, seed=rank, face_size=S)
+            prefix = serve.make_stream(m, args.serve_rate, seed=0, face_size=S)
             out["serial_fp32_prefix"] = serve.serve_serial(e, frames, base, prefix, precision="fp32")
         e.close()
         del frames, base
         torch.cuda.empty_cache()
     if rank == 0:
-        s = out.get("served_bf16") or out["served_bf16_small_net"]
+        s_ = out.get("served_bf16") or out["served_bf16_small_net"]
         line = {"metric": f"p99 relight latency, {args.serve_requests} requests Poisson {args.serve_rate:g}/s",
-                "value": s["p99_ms"], "unit": "ms", "n_gpus": world, "steps": 1, "warmup": 0,
-                "ms_per_step": s["makespan_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+                "value": s_["p99_ms"], "unit": "ms", "n_gpus": world, "steps": 1, "warmup": 0,
+                "ms_per_step": s_["makespan_s"] * 1e3, "higher_is_better": False, "scaling": "strong",
                 "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
                 "config": {"workload": "serving stream: resolutions {256^2, 512^2, 720p, 1080p, 1440p}, "
                                        "K in {64,128,300}, 40% new 6x64x64 env maps, 60% rotations, "
-                                       f"150 GB admission budget, {args.serve_quantum_ms:g} ms quanta",
-                           "networks": args.serve_nets},
+                                       f"150 GB admission budget, {args.serve_quantum_ms:g} ms quanta, "
+                                       f"order {args.serve_order}{', adaptive quanta' if args.serve_adaptive else ''}",
+                           "networks": args.serve_nets,
+                           "parallelism": f"request-dp{world} with row-band splits" if world > 1 else "1 GPU"},
                 "clocks": clocks, **out}
         print(json.dumps(line), flush=True)
+    if channels is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------- precision sweep

@@ -65,6 +65,32 @@ def local_requests(requests: Sequence[Request], plan: Sequence[Tuple[int, bool]]
     return mine
 
 
+class _Transfer:
+    """A posted send or receive that can be polled.  NCCL's work objects report completion
+    through a CUDA event (``is_completed``); gloo's complete only inside ``wait``, so on CPU
+    ranks a helper thread waits and raises a flag."""
+
+    def __init__(self, work, threaded: bool):
+        self.work = work
+        self.ok = True
+        self.flag = None
+        if threaded:
+            import threading
+            self.flag = threading.Event()
+            threading.Thread(target=self._wait, daemon=True).start()
+
+    def _wait(self):
+        try:
+            self.work.wait()
+        except Exception:
+            self.ok = False
+        finally:
+            self.flag.set()
+
+    def is_completed(self) -> bool:
+        return self.flag.is_set() if self.flag is not None else self.work.is_completed()
+
+
 class PairChannels:
     """One process group per direction of every pair of ranks, for the band transfers.
 
@@ -77,17 +103,18 @@ class PairChannels:
     def __init__(self, world: int):
         import torch.distributed as dist
         self.dist = dist
+        self.threaded = dist.get_backend() == "gloo"
         self.groups = {}
         for a in range(world):
             for b in range(a + 1, world):
                 self.groups[(a, b)] = dist.new_group([a, b])
                 self.groups[(b, a)] = dist.new_group([a, b])
 
-    def isend(self, t, src: int, dst: int):
-        return self.dist.isend(t, dst=dst, group=self.groups[(src, dst)])
+    def isend(self, t, src: int, dst: int) -> _Transfer:
+        return _Transfer(self.dist.isend(t, dst=dst, group=self.groups[(src, dst)]), self.threaded)
 
-    def irecv(self, t, src: int, dst: int):
-        return self.dist.irecv(t, src=src, group=self.groups[(src, dst)])
+    def irecv(self, t, src: int, dst: int) -> _Transfer:
+        return _Transfer(self.dist.irecv(t, src=src, group=self.groups[(src, dst)]), self.threaded)
 
 
 class BandGather(LocalCompletion):
@@ -206,7 +233,7 @@ class BandGather(LocalCompletion):
                 continue
             del self.recvs[rid]
             r = self.req[rid]
-            bad = sum(int(flag.item()) == 0 for _, flag, _ in parts)
+            bad = sum(int(flag.item()) == 0 or not all(w.ok for w in works) for works, flag, _ in parts)
             if self.local.pop(rid) and r.status == "gathering":
                 if bad:
                     self.band_failures[rid] = bad
@@ -232,8 +259,11 @@ def serve_distributed(engine, frames, base_faces, requests: Sequence[Request], r
     gather = BandGather(rank, world, mine, frame_dims, channels, device)
     srv = RelightServer(engine, frames, base_faces, completion=gather, **(server_kwargs or {}))
     summ = srv.run(mine, realtime=realtime)
+    for r in mine:  # a split request with a band that failed on another rank failed as a whole
+        if gather.band_failures.get(r.rid) and r.owner == rank:
+            r.status = "error"
     owned = [r for r in mine if r.owner == rank or not r.split]
-    done = [r for r in owned if r.status == "done" and not gather.band_failures.get(r.rid)]
+    done = [r for r in owned if r.status == "done"]
     summ["latency_ms"] = [r.latency * 1e3 for r in done]
     summ["owned"] = len(owned)
     summ["owned_done"] = len(done)

@@ -6,7 +6,9 @@ while a device-memory budget allows (their output buffers and env tables), and f
 GPU fixed-size *quanta* of work: each quantum is one ``nwprt_relight_ranges`` launch that
 packs 128-pixel-aligned pixel ranges of several admitted requests, in arrival order
 (``order="fifo"``, the default: it gives the lower p99) or smallest remaining work first
-(``order="srpt"``: lower p50 when the stream overloads the GPU).  Requests that arrive while
+(``order="srpt"``: lower p50 when the stream overloads the GPU), or earliest deadline first
+(``order="edf"``: a deadline proportional to each request's own size, so that small requests
+are not queued behind large ones).  Requests that arrive while
 quanta are running join the next quantum, and two quanta are kept in flight so the GPU does
 not idle while the host forms the next one.
 
@@ -125,14 +127,28 @@ class Admission:
         assert self.used >= 0
 
 
-def plan_quantum(active: Sequence[Request], quantum_evals: int, order: str = "srpt") -> List[Tuple[Request, int, int]]:
-    """Chunks for one launch: requests in order of least remaining work ("srpt") or of
-    arrival ("fifo"), each chunk a 128-pixel-aligned range, until the quantum is full.
-    Always makes progress: the first request gets at least one tile even if that alone
-    exceeds the quantum."""
-    if order not in ("srpt", "fifo"):
+def deadline(r: Request, evals_per_s: float, slack: float = 4.0, floor_s: float = 0.016) -> float:
+    """Target completion time of a request for earliest-deadline-first packing: its arrival
+    plus `slack` times its own service time alone (pixels x K at `evals_per_s`), and never
+    less than `floor_s` -- small requests get tight deadlines, large ones loose ones."""
+    px = (r.n_px - max(0, r.px_lo)) if r.n_px else 0
+    return r.arrival + max(floor_s, slack * px * r.K / evals_per_s)
+
+
+def plan_quantum(active: Sequence[Request], quantum_evals: int, order: str = "srpt",
+                 evals_per_s: float = 1e10) -> List[Tuple[Request, int, int]]:
+    """Chunks for one launch: requests in order of least remaining work ("srpt"), of
+    arrival ("fifo") or of deadline ("edf", see ``deadline``), each chunk a 128-pixel-aligned
+    range, until the quantum is full.  Always makes progress: the first request gets at
+    least one tile even if that alone exceeds the quantum."""
+    if order not in ("srpt", "fifo", "edf"):
         raise ValueError(f"unknown quantum order {order!r}")
-    key = (lambda r: (r.remaining_evals, r.rid)) if order == "srpt" else (lambda r: (r.arrival, r.rid))
+    if order == "srpt":
+        key = lambda r: (r.remaining_evals, r.rid)
+    elif order == "fifo":
+        key = lambda r: (r.arrival, r.rid)
+    else:
+        key = lambda r: (deadline(r, evals_per_s), r.rid)
     plan = []
     used = 0
     for r in sorted((r for r in active if r.next_px < r.n_px), key=key):
@@ -233,7 +249,8 @@ class RelightServer:
                  quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
                  max_in_flight: int = 2, keep_outputs: bool = False,
                  fault: Optional[Callable[[Request, str], Optional[str]]] = None,
-                 max_active: Optional[int] = None, order: str = "fifo", completion=None):
+                 max_active: Optional[int] = None, order: str = "fifo", completion=None,
+                 adaptive_quantum: bool = False):
         import torch
         self.torch = torch
         self.e = engine
@@ -242,7 +259,11 @@ class RelightServer:
         from .engine import RenderConfig
         self.cfg = RenderConfig(precision=precision)
         self.adm = Admission(budget_bytes)
+        self.rate = est_evals_per_s
         self.quantum = int(est_evals_per_s * quantum_ms / 1e3)
+        # with adaptive quanta, a request admitted more than one quantum ago and not yet
+        # started shrinks the next quantum (down to a quarter) so that it starts sooner
+        self.adaptive = adaptive_quantum
         self.max_queue_s = max_queue_s
         self.max_in_flight = max_in_flight
         # admission also stops at max_active admitted requests (None: the byte budget alone)
@@ -262,7 +283,9 @@ class RelightServer:
         """Output buffers and the env wavelet table, stream-ordered before its first quantum."""
         torch = self.torch
         fr = self.frames[r.res]
-        ind = torch.empty((r.n_px, 4), dtype=torch.float32, device=fr.fbPredictedIndirect.device)
+        # outputs are indexed by absolute pixel: a band's buffer covers the whole frame, which
+        # also lets a split request's owner receive the other ranks' bands into it
+        ind = torch.empty((fr.width * fr.height, 4), dtype=torch.float32, device=fr.fbPredictedIndirect.device)
         wd = torch.empty_like(ind)
         if r.env_kind == "new":
             faces = torch.from_numpy(np.ascontiguousarray(r.faces, np.float32)).to(ind.device, non_blocking=True)
@@ -303,6 +326,15 @@ class RelightServer:
                 except Exception:
                     failed.append(r)
             return failed
+
+    def _quantum_now(self, active: Sequence[Request], t: float) -> int:
+        if not self.adaptive:
+            return self.quantum
+        q_s = self.quantum / self.rate
+        waiting = [t - r.t_admit for r in active if r.next_px == max(0, r.px_lo)]
+        if waiting and max(waiting) > q_s:
+            return max(self.quantum // 4, int(self.quantum * q_s / max(waiting)))
+        return self.quantum
 
     def _retire(self, r: Request, t: float) -> None:
         """A request whose work (and gather) is complete: returns its budget and env table."""
@@ -360,7 +392,8 @@ class RelightServer:
                     self._refuse(r, "error", now())
                     finished += 1
                     continue
-                nbytes = request_bytes(r.n_px, r.K, self.face_size, self.enc_dims)
+                fr = self.frames[r.res]
+                nbytes = request_bytes(fr.width * fr.height, r.K, self.face_size, self.enc_dims)
                 if nbytes > self.adm.budget:
                     queue.popleft()
                     self._refuse(r, "rejected", now())
@@ -389,7 +422,7 @@ class RelightServer:
                 active.append(r)
             self.max_active = max(self.max_active, len(active))
             if active and len(in_flight) < self.max_in_flight:
-                plan = plan_quantum(active, self.quantum, self.order)
+                plan = plan_quantum(active, self._quantum_now(active, now()), self.order, self.rate)
                 launch = []
                 for r, b, e in plan:
                     try:
@@ -403,9 +436,11 @@ class RelightServer:
                     launch.append((r, (r.env_id, r.res, r.outputs[0], r.outputs[1], b, e), e))
                 if not launch:
                     continue
-                torch.cuda.nvtx.range_push(f"quantum {self.quanta}: {len(launch)} requests")
+                if self.on_gpu:
+                    torch.cuda.nvtx.range_push(f"quantum {self.quanta}: {len(launch)} requests")
                 failed = self._launch([(r, rg) for r, rg, _ in launch])
-                torch.cuda.nvtx.range_pop()
+                if self.on_gpu:
+                    torch.cuda.nvtx.range_pop()
                 for r in failed:
                     active.remove(r)
                     self._end_failed(r, now())
@@ -447,10 +482,23 @@ class RelightServer:
         return summarize(requests, now())
 
 
+# latency classes of the serving stream: resolutions up to 1280x720, and larger ones
+SMALL_CLASS_MAX_PX = 1280 * 720
+
+
+def class_latency(requests: Sequence[Request], frame_px: Sequence[int]) -> Dict:
+    """p50 / p99 of the finished requests per class (small: <= 720p frames, large: above)."""
+    out = {}
+    for name, pick in (("small", lambda n: n <= SMALL_CLASS_MAX_PX), ("large", lambda n: n > SMALL_CLASS_MAX_PX)):
+        lat = [r.latency * 1e3 for r in requests if r.status == "done" and pick(frame_px[r.res])]
+        out[name] = {"done": len(lat), "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99)}
+    return out
+
+
 def summarize(requests: Sequence[Request], makespan: float) -> Dict:
     done = [r for r in requests if r.status == "done"]
     lat = [r.latency * 1e3 for r in done]
-    evals = sum(r.n_px * r.K for r in done)
+    evals = sum((r.n_px - max(0, r.px_lo)) * r.K for r in done)
     return {
         "requests": len(requests),
         "done": len(done),

@@ -226,3 +226,35 @@ def test_injected_faults_stay_with_their_requests(rig):
         if r.status == "done":
             ind, wd = _solo(e, frames, base, r)
             assert torch.equal(r.outputs[0], ind) and torch.equal(r.outputs[1], wd), r.rid
+
+
+@pytest.mark.parametrize("order,adaptive", [("edf", False), ("edf", True), ("srpt", True)])
+def test_packing_orders_keep_results(rig, order, adaptive):
+    import torch
+    e, frames, base = rig
+    reqs = _requests(10, seed=7)
+    srv = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=0.05, est_evals_per_s=9e9,
+                              keep_outputs=True, order=order, adaptive_quantum=adaptive)
+    stats = srv.run(reqs)
+    assert stats["done"] == len(reqs), stats
+    for r in reqs:
+        ind, _ = _solo(e, frames, base, r)
+        assert torch.equal(r.outputs[0], ind), (order, r.rid)
+    cls = serve.class_latency(reqs, [f.width * f.height for f in frames])
+    assert cls["small"]["done"] == len(reqs)
+
+
+def test_dispatcher_on_one_gpu(rig):
+    """The multi-GPU dispatcher at world size 1: every request placed on rank 0, none split,
+    results equal to the same requests relit alone."""
+    import torch
+    from neural_wavelet_prt_demo_b200 import dispatch
+    e, frames, base = rig
+    reqs = _requests(8, seed=9)
+    summ = dispatch.serve_distributed(e, frames, base, reqs, 0, 1, None, "cuda", evals_per_s=9e9,
+                                      server_kwargs=dict(precision="bf16", quantum_ms=0.05, est_evals_per_s=9e9,
+                                                         keep_outputs=True))
+    assert summ["owned_done"] == len(reqs) and summ["split_requests"] == 0
+    for r in summ["local"]:
+        ind, _ = _solo(e, frames, base, r)
+        assert torch.equal(r.outputs[0], ind), r.rid
