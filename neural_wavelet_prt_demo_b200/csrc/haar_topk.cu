@@ -31,6 +31,8 @@
 //    their outputs.
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include "nwprt_internal.cuh"
 
 namespace cg = cooperative_groups;
@@ -171,34 +173,49 @@ __device__ __forceinline__ void shuffle_level(float ll[3], int lane, int s, int 
   }
 }
 
+// Geometry of one face's transform: thread t < T owns the B x B texel block at Morton(t).
 template <int S>
-__global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
-    haar_topk_kernel(const float* __restrict__ faces, int K, int32_t* __restrict__ idx_out,
-                     float* __restrict__ st_out) {
-  constexpr int B = S < 4 ? S : 4;   // texel block per thread: B x B
-  constexpr int G = S / B;           // thread blocks per face side; the upper block is G x G
-  constexpr int T = G * G;           // threads holding coefficients
-  constexpr int SS = S * S;
-  constexpr int NR = B == 4 ? 15 : (B == 2 ? 3 : 0);  // coefficients held in registers
-  constexpr int NW = (SS + 31) / 32;
-  static_assert(T <= kThreads, "one 4x4 block per thread");
+struct FaceGeom {
+  static constexpr int B = S < 4 ? S : 4;   // texel block per thread: B x B
+  static constexpr int G = S / B;           // thread blocks per face side; the upper block is G x G
+  static constexpr int T = G * G;           // threads holding coefficients
+  static constexpr int SS = S * S;
+  static constexpr int NR = B == 4 ? 15 : (B == 2 ? 3 : 0);  // coefficients held in registers
+  static constexpr int NK = NR + 1;                         // plus one entry of the upper block
+};
 
-  extern __shared__ __align__(16) char smem_raw[];
-  HaarSmem sm;
-  smem_layout(S, K, smem_raw, &sm);
-  cg::cluster_group cluster = cg::this_cluster();
-  const int face = (int)cluster.block_rank();
-  const int env = blockIdx.x / 6;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const float* src = faces + ((size_t)env * 6 + face) * (size_t)SS * 3;
+// Index within the face of thread tid's coefficient u (u == NR: its upper-block entry).
+template <int S>
+__device__ __forceinline__ int flat_in_face(int tid, int u) {
+  using F = FaceGeom<S>;
+  if (u == F::NR) return (tid / F::G) * S + (tid % F::G);
+  int i = 0, j = 0, h = 1;
+  if constexpr (F::B == 4) {
+    const int bj = morton_even(tid), bi = morton_even(tid >> 1);
+    const int q = u / 3;
+    i = q < 4 ? 2 * bi + (q >> 1) : bi;
+    j = q < 4 ? 2 * bj + (q & 1) : bj;
+    h = q < 4 ? S / 2 : S / 4;
+  }
+  const int band = u % 3;
+  return band == 0 ? i * S + j + h : (band == 1 ? (i + h) * S + j : (i + h) * S + j + h);
+}
+
+// The full Haar transform of one face [S][S][3] at `src` by the block's kThreads threads:
+// levels 1-2 on each thread's B x B block in registers (co: its NR detail coefficients),
+// the next levels by warp shuffles, the last ones in warp 0.  The G x G upper block of the
+// result (levels >= 3 and the DC term) lands in `upper` [G*G][3]; `llg` is [16][3] staging.
+// Ends with a block barrier, after which `upper` is complete.
+template <int S>
+__device__ __forceinline__ void haar_face_in_registers(const float* __restrict__ src, int tid,
+                                                       float (&co)[FaceGeom<S>::NR > 0 ? FaceGeom<S>::NR : 1][3],
+                                                       float* upper, float* llg) {
+  using F = FaceGeom<S>;
+  constexpr int B = F::B, G = F::G, T = F::T, NR = F::NR;
+  const int lane = tid & 31, warp = tid >> 5;
   const bool owner = tid < T;
   const int bj = morton_even(tid), bi = morton_even(tid >> 1);
-
-  if (face == 0 && tid == 0) sm.scal[kScCounter] = 0;  // winner slots (read after 5 cluster barriers)
-  for (int w = tid; w < NW; w += kThreads) sm.bits[w] = 0u;
-
   // ---- levels 1 and 2 on this thread's B x B block, in registers
-  float co[NR > 0 ? NR : 1][3];  // detail coefficients held in registers (RGB)
 #pragma unroll
   for (int u = 0; u < (NR > 0 ? NR : 1); ++u) co[u][0] = co[u][1] = co[u][2] = 0.f;
   float ll[3] = {0.f, 0.f, 0.f};
@@ -274,7 +291,7 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
 #pragma unroll
     for (int lev = 0; lev < 2; ++lev)
       if (n >= 2) {
-        shuffle_level(ll, lane, s, tid / (4 * s), n / 2, owner, sm.upper, G);
+        shuffle_level(ll, lane, s, tid / (4 * s), n / 2, owner, upper, G);
         n /= 2;
         s *= 4;
       }
@@ -282,45 +299,60 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
       // at most 4 x 4 values left: leaders hand them to warp 0
       if (owner && (tid & (s - 1)) == 0)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) sm.llg[(tid / s) * 3 + c] = ll[c];
+        for (int c = 0; c < 3; ++c) llg[(tid / s) * 3 + c] = ll[c];
       __syncthreads();
       if (warp == 0) {
         const bool live = lane < n * n;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) ll[c] = live ? sm.llg[lane * 3 + c] : 0.f;
+        for (int c = 0; c < 3; ++c) ll[c] = live ? llg[lane * 3 + c] : 0.f;
         int s2 = 1;
 #pragma unroll
         for (int lev = 0; lev < 2; ++lev)
           if (n >= 2) {
-            shuffle_level(ll, lane, s2, lane / (4 * s2), n / 2, live, sm.upper, G);
+            shuffle_level(ll, lane, s2, lane / (4 * s2), n / 2, live, upper, G);
             n /= 2;
             s2 *= 4;
           }
         if (lane == 0)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) sm.upper[c] = ll[c];
+          for (int c = 0; c < 3; ++c) upper[c] = ll[c];
       }
     } else if (tid == 0) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) sm.upper[c] = ll[c];
+      for (int c = 0; c < 3; ++c) upper[c] = ll[c];
     }
   }
   __syncthreads();
+}
+
+template <int S>
+__global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
+    haar_topk_kernel(const float* __restrict__ faces, int K, int32_t* __restrict__ idx_out,
+                     float* __restrict__ st_out) {
+  using F = FaceGeom<S>;
+  constexpr int T = F::T, SS = F::SS, NR = F::NR;
+  constexpr int NW = (SS + 31) / 32;
+  static_assert(T <= kThreads, "one 4x4 block per thread");
+
+  extern __shared__ __align__(16) char smem_raw[];
+  HaarSmem sm;
+  smem_layout(S, K, smem_raw, &sm);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int face = (int)cluster.block_rank();
+  const int env = blockIdx.x / 6;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const float* src = faces + ((size_t)env * 6 + face) * (size_t)SS * 3;
+  const bool owner = tid < T;
+
+  if (face == 0 && tid == 0) sm.scal[kScCounter] = 0;  // winner slots (read after 5 cluster barriers)
+  for (int w = tid; w < NW; w += kThreads) sm.bits[w] = 0u;
+
+  // ---- the transform: levels 1-2 in registers, the rest by shuffles and warp 0
+  float co[NR > 0 ? NR : 1][3];  // detail coefficients held in registers (RGB)
+  haar_face_in_registers<S>(src, tid, co, sm.upper, sm.llg);
   // ---- this thread's 16 coefficients: NR in registers, one of the upper block
-  constexpr int NK = NR + 1;
-  // index within the face of this thread's coefficient u (u == NR: its upper-block entry)
-  auto flat_of = [&](int u) -> int {
-    if (u == NR) return (tid / G) * S + (tid % G);
-    int i = 0, j = 0, h = 1;
-    if constexpr (B == 4) {
-      const int q = u / 3;
-      i = q < 4 ? 2 * bi + (q >> 1) : bi;
-      j = q < 4 ? 2 * bj + (q & 1) : bj;
-      h = q < 4 ? S / 2 : S / 4;
-    }
-    const int band = u % 3;
-    return band == 0 ? i * S + j + h : (band == 1 ? (i + h) * S + j : (i + h) * S + j + h);
-  };
+  constexpr int NK = F::NK;
+  auto flat_of = [&](int u) -> int { return flat_in_face<S>(tid, u); };
   uint32_t key[NK];
 #pragma unroll
   for (int u = 0; u < NR; ++u) key[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
@@ -453,8 +485,296 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
   }
 }
 
+// ------------------------------------------------------------------ batched form
+// One persistent CTA per map at a time (no cluster): for large batches, whole maps in flight
+// per SM beat the cluster's one sixth of a map each, and no step crosses an SM.  Faces are
+// transformed one after another with the same register code; the keys of all six stay in
+// shared memory (uint4 of four keys, thread-fastest: conflict-free), the coefficients go to
+// this CTA's slice of a global scratch buffer ([face][u][channel][thread], coalesced; it
+// stays in L2 because every CTA reuses its own slice map after map).  The select is the
+// cluster form's, block-local: per-warp histograms, a bitmap of ties over the 6*S*S flat
+// indices, winner slots from one block scan, and a rank by broadcast reads of the K keys.
+
+struct BatchSmem {
+  uint4* keys;      // [6][NK/4][kThreads]
+  uint32_t* whist;  // [kWarps][256] per-warp histograms of a pass
+  uint32_t* bits;   // [6*S*S/32] ties (aliases whist after the passes)
+  uint32_t* wpre;   // [6*S*S/32]
+  uint64_t* gkey;   // [K]
+  int* gid;         // [K] winner: (face * NK + u) * kThreads + thread
+  float* upper;     // [(S/4)^2][3]
+  float* llg;       // [16][3]
+  int* warp_tot;
+  int* scal;
+};
+
+__host__ __device__ inline size_t batch_smem_layout(int S, int K, char* base, BatchSmem* L) {
+  const int G = S < 4 ? 1 : S / 4;
+  const int nk = S >= 4 ? 16 : (S == 2 ? 4 : 1);
+  const int nkq = (nk + 3) / 4;
+  const int nw = (6 * S * S + 31) / 32;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o = align16(o + bytes); return at; };
+  const size_t oK = take(sizeof(uint4) * 6 * nkq * kThreads);
+  const size_t uA = sizeof(uint32_t) * kWarps * 256, uB = sizeof(uint32_t) * 2 * nw;
+  const size_t oH = take(uA > uB ? uA : uB);
+  const size_t oG = take(sizeof(uint64_t) * K);
+  const size_t oI = take(sizeof(int) * K);
+  const size_t oU = take(sizeof(float) * 3 * G * G);
+  const size_t oL = take(sizeof(float) * 3 * 16);
+  const size_t oW = take(sizeof(int) * kWarps);
+  const size_t oS = take(sizeof(int) * 32);
+  if (L) {
+    L->keys = (uint4*)(base + oK);
+    L->whist = (uint32_t*)(base + oH);
+    L->bits = (uint32_t*)(base + oH);
+    L->wpre = (uint32_t*)(base + oH) + nw;
+    L->gkey = (uint64_t*)(base + oG);
+    L->gid = (int*)(base + oI);
+    L->upper = (float*)(base + oU);
+    L->llg = (float*)(base + oL);
+    L->warp_tot = (int*)(base + oW);
+    L->scal = (int*)(base + oS);
+  }
+  return o;
+}
+
+template <int S>
+constexpr size_t batch_scratch_floats_per_cta() {
+  return (size_t)6 * FaceGeom<S>::NK * 3 * kThreads;
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads, 2)
+    haar_topk_batch_kernel(const float* __restrict__ faces, int n_env, int K, int32_t* __restrict__ idx_out,
+                           float* __restrict__ st_out, float* __restrict__ scratch) {
+  using F = FaceGeom<S>;
+  constexpr int T = F::T, SS = F::SS, NR = F::NR, NK = F::NK;
+  constexpr int NKQ = (NK + 3) / 4;
+  constexpr int NW = (6 * SS + 31) / 32;
+  static_assert(T <= kThreads, "one 4x4 block per thread");
+  extern __shared__ __align__(16) char smem_raw[];
+  BatchSmem sm;
+  batch_smem_layout(S, K, smem_raw, &sm);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool owner = tid < T;
+  float* rgb = scratch + (size_t)blockIdx.x * batch_scratch_floats_per_cta<S>();
+  // [face][u][channel][thread]
+  auto rgb_at = [&](int f, int u, int c, int t) -> float* { return rgb + (((size_t)f * NK + u) * 3 + c) * kThreads + t; };
+
+  for (int env = blockIdx.x; env < n_env; env += gridDim.x) {
+    // ---- the six transforms: keys to shared memory, coefficients to the scratch slice
+    for (int f = 0; f < 6; ++f) {
+      const float* src = faces + ((size_t)env * 6 + f) * (size_t)SS * 3;
+      float co[NR > 0 ? NR : 1][3];
+      haar_face_in_registers<S>(src, tid, co, sm.upper, sm.llg);
+      uint32_t k[NKQ * 4];
+#pragma unroll
+      for (int u = 0; u < NKQ * 4; ++u) k[u] = 0u;
+      if (owner) {
+#pragma unroll
+        for (int u = 0; u < NR; ++u) {
+          k[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) *rgb_at(f, u, c, tid) = co[u][c];
+        }
+        const float ur = sm.upper[tid * 3], ug = sm.upper[tid * 3 + 1], ub = sm.upper[tid * 3 + 2];
+        k[NR] = wavelet_key_bits(ur, ug, ub);
+        *rgb_at(f, NR, 0, tid) = ur;
+        *rgb_at(f, NR, 1, tid) = ug;
+        *rgb_at(f, NR, 2, tid) = ub;
+      }
+#pragma unroll
+      for (int q = 0; q < NKQ; ++q)
+        sm.keys[((size_t)f * NKQ + q) * kThreads + tid] = make_uint4(k[4 * q], k[4 * q + 1], k[4 * q + 2], k[4 * q + 3]);
+      __syncthreads();  // the next face reuses `upper`
+    }
+    // ---- 4-pass radix select of the K-th largest key
+    uint32_t prefix = 0, mask = 0;
+    int remaining = K;
+    for (int pass = 0; pass < 4; ++pass) {
+      const int shift = 24 - 8 * pass;
+      for (int i = tid; i < kWarps * 256; i += kThreads) sm.whist[i] = 0u;
+      __syncthreads();
+      if (owner) {
+        uint32_t* h = sm.whist + warp * 256;
+        for (int f = 0; f < 6; ++f)
+#pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (4 * q + i < NK && (kk[i] & mask) == prefix) atomicAdd(&h[(kk[i] >> shift) & 255u], 1u);
+          }
+      }
+      __syncthreads();
+      const int digit = 255 - tid;
+      uint32_t tot = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) tot += sm.whist[w * 256 + digit];
+      uint32_t all;
+      const uint32_t incl = block_inclusive_sum(tot, sm.warp_tot, &all);
+      if (incl >= (uint32_t)remaining && incl - tot < (uint32_t)remaining) {
+        sm.scal[kScPrefix] = (int)(prefix | ((uint32_t)digit << shift));
+        sm.scal[kScMask] = (int)(mask | (255u << shift));
+        sm.scal[kScRemaining] = remaining - (int)(incl - tot);
+      }
+      __syncthreads();
+      prefix = (uint32_t)sm.scal[kScPrefix];
+      mask = (uint32_t)sm.scal[kScMask];
+      remaining = sm.scal[kScRemaining];
+    }
+    // ---- ties at the threshold in flat-index order: a bitmap over face * S*S + flat
+    const uint32_t thr = prefix;
+    for (int w = tid; w < NW; w += kThreads) sm.bits[w] = 0u;
+    __syncthreads();
+    if (owner)
+      for (int f = 0; f < 6; ++f)
+#pragma unroll
+        for (int q = 0; q < NKQ; ++q) {
+          const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+          const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (4 * q + i < NK && kk[i] == thr) {
+              const int g = f * SS + flat_in_face<S>(tid, 4 * q + i);
+              atomicOr(&sm.bits[g >> 5], 1u << (g & 31));
+            }
+        }
+    __syncthreads();
+    {
+      // exclusive popcount prefix over the bitmap: thread t covers words [t*per, t*per + per)
+      constexpr int PER = (NW + kThreads - 1) / kThreads;
+      uint32_t pc[PER], mine = 0;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int w = tid * PER + i;
+        pc[i] = w < NW ? (uint32_t)__popc(sm.bits[w]) : 0u;
+        mine += pc[i];
+      }
+      uint32_t all;
+      uint32_t run = block_inclusive_sum(mine, sm.warp_tot, &all) - mine;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int w = tid * PER + i;
+        if (w < NW) sm.wpre[w] = run;
+        run += pc[i];
+      }
+    }
+    __syncthreads();
+    // ---- winners: slots from one block scan of per-thread counts
+    int n_sel = 0;
+    if (owner)
+      for (int f = 0; f < 6; ++f)
+#pragma unroll
+        for (int q = 0; q < NKQ; ++q) {
+          const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+          const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (4 * q + i >= NK) continue;
+            bool sel = kk[i] > thr;
+            if (kk[i] == thr) {
+              const int g = f * SS + flat_in_face<S>(tid, 4 * q + i), w = g >> 5;
+              sel = (int)(sm.wpre[w] + __popc(sm.bits[w] & ((1u << (g & 31)) - 1u))) < remaining;
+            }
+            n_sel += sel;
+          }
+        }
+    uint32_t all_sel;
+    int slot = (int)block_inclusive_sum((uint32_t)n_sel, sm.warp_tot, &all_sel) - n_sel;
+    if (owner && n_sel)
+      for (int f = 0; f < 6; ++f)
+#pragma unroll
+        for (int q = 0; q < NKQ; ++q) {
+          const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+          const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (4 * q + i >= NK) continue;
+            const int u = 4 * q + i;
+            const int g = f * SS + flat_in_face<S>(tid, u);
+            bool sel = kk[i] > thr;
+            if (kk[i] == thr) {
+              const int w = g >> 5;
+              sel = (int)(sm.wpre[w] + __popc(sm.bits[w] & ((1u << (g & 31)) - 1u))) < remaining;
+            }
+            if (sel) {
+              sm.gkey[slot] = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
+              sm.gid[slot] = (f * NK + u) * kThreads + tid;
+              ++slot;
+            }
+          }
+        }
+    __syncthreads();
+    // ---- rank the K winners (broadcast reads of the composite keys) and write them out
+    for (int e = tid; e < K; e += kThreads) {
+      const uint64_t me = sm.gkey[e];
+      int rank = 0;
+      for (int o = 0; o < K; ++o) rank += sm.gkey[o] > me;
+      const int id = sm.gid[e];
+      const int t = id % kThreads, fu = id / kThreads, f = fu / NK, u = fu % NK;
+      const size_t out = (size_t)env * K + rank;
+      idx_out[out] = f * SS + flat_in_face<S>(t, u);
+      st_out[out * 3 + 0] = *rgb_at(f, u, 0, t);
+      st_out[out * 3 + 1] = *rgb_at(f, u, 1, t);
+      st_out[out * 3 + 2] = *rgb_at(f, u, 2, t);
+    }
+    __syncthreads();  // the next map reuses every shared array and the scratch slice
+  }
+}
+
+// Batches of at least this many maps use the batched kernel; smaller ones the cluster form,
+// whose six CTAs per map give the lower latency for a single map.
+constexpr int kBatchMinMaps = 32;
+
+// A stream-ordered pool per device for the batched kernel's scratch.  It keeps its memory
+// between calls (release threshold = max), so a steady stream of batches allocates once.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64] = {};
+
+cudaMemPool_t scratch_pool(int dev) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (dev < 0 || dev >= 64) fail(NWPRT_UNSUPPORTED, "haar_topk: device ordinal beyond the pool table");
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    NWPRT_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~0ull;
+    NWPRT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pool[dev] = pool;
+  }
+  return g_pool[dev];
+}
+
 template <int S>
 void launch_s(const float* faces, int n_env, int K, int32_t* idx, float* strength, cudaStream_t st) {
+  int dev = 0, sms = 0, max_smem = 0;
+  NWPRT_CUDA(cudaGetDevice(&dev));
+  NWPRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  NWPRT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t bsmem = batch_smem_layout(S, K, nullptr, nullptr);
+  if (n_env >= kBatchMinMaps && bsmem <= (size_t)max_smem) {
+    NWPRT_CUDA(cudaFuncSetAttribute(haar_topk_batch_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+    int per_sm = 0;
+    NWPRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, haar_topk_batch_kernel<S>, kThreads, bsmem));
+    const long long slots = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(n_env < slots ? n_env : slots);
+    void* scratch = nullptr;
+    const size_t bytes = (size_t)grid * batch_scratch_floats_per_cta<S>() * sizeof(float);
+    if (cudaMallocFromPoolAsync(&scratch, bytes, scratch_pool(dev), st) == cudaSuccess) {
+      haar_topk_batch_kernel<S><<<grid, kThreads, bsmem, st>>>(faces, n_env, K, idx, strength, (float*)scratch);
+      const cudaError_t launch = cudaGetLastError();
+      NWPRT_CUDA(cudaFreeAsync(scratch, st));
+      NWPRT_CUDA(launch);
+      return;
+    }
+    (void)cudaGetLastError();  // no scratch: the cluster form needs none
+  }
   const size_t smem = smem_layout(S, K, nullptr, nullptr);
   NWPRT_CUDA(cudaFuncSetAttribute(haar_topk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   haar_topk_kernel<S><<<6 * n_env, kThreads, smem, st>>>(faces, K, idx, strength);

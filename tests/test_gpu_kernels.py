@@ -52,6 +52,30 @@ def test_haar_topk_large_batch(cuda):
     assert np.array_equal(st.cpu().numpy().view(np.uint32), rst.view(np.uint32))
 
 
+@pytest.mark.parametrize("S,K", [(64, 300), (64, 1024), (32, 64), (8, 384), (4, 17), (2, 24), (1, 6)])
+def test_haar_topk_batched_and_single_map_forms_agree(cuda, S, K):
+    """Batches of 32 maps or more run the batched kernel (one CTA per map), single maps the
+    cluster kernel (one CTA per face): both give the oracle's bits, ties and non-finite
+    texels included."""
+    import torch
+    E = 40
+    g = np.random.default_rng(S + K)
+    faces = np.stack([synth.make_env_faces(S, seed=5, index=e) for e in range(E)])
+    faces[3] = g.integers(0, 3, size=(6, S, S, 3)).astype(np.float32)   # many equal keys
+    faces[7] = 1.0                                                      # constant map
+    faces[9, 1, 0, 0, 0] = np.nan
+    faces[11, 4, S - 1, S - 1, 2] = np.inf
+    tf = torch.from_numpy(faces).to(cuda)
+    idx, st = _engine().haar_topk(tf, K)
+    ridx, rst = O.haar_topk(faces, K)
+    assert np.array_equal(idx.cpu().numpy(), ridx)
+    assert bits_equal(st.cpu().numpy(), rst)
+    for e in (0, 3, 7, 9, 11, E - 1):
+        i1, s1 = _engine().haar_topk(tf[e:e + 1].contiguous(), K)
+        assert np.array_equal(i1.cpu().numpy()[0], ridx[e]), e
+        assert bits_equal(s1.cpu().numpy()[0], rst[e]), e
+
+
 def test_haar_topk_rejects_bad_sizes(cuda):
     import torch
     eng = _engine()
