@@ -57,11 +57,9 @@ def parse_args():
                     help="serve: kernel time per scheduling quantum")
     ap.add_argument("--serve-nets", choices=["both", "large", "small"], default="both",
                     help="serve: which network(s) to run (config 2, config 0, or both)")
-    ap.add_argument("--serve-order", choices=["fifo", "srpt", "edf"], default="fifo",
-                    help="serve: quantum packing order (arrival, least remaining work, or earliest "
-                         "deadline with deadlines proportional to request size)")
-    ap.add_argument("--serve-adaptive", action="store_true",
-                    help="serve: shrink a quantum when an admitted request has not started within one")
+    ap.add_argument("--serve-order", choices=["fifo", "srpt", "edf"], default="edf",
+                    help="serve: quantum packing order (earliest deadline with deadlines proportional to "
+                         "request size, arrival, or least remaining work)")
     ap.add_argument("--serve-max-active", type=int, default=0,
                     help="serve: admit at most this many requests at once (0: the byte budget alone)")
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
@@ -795,8 +793,7 @@ def run_serve(args, rank, world, local, dev):
             rate = float(t.item())
         reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=0, face_size=S)
         kw = dict(precision="bf16", budget_bytes=150 << 30, quantum_ms=args.serve_quantum_ms, est_evals_per_s=rate,
-                  max_active=args.serve_max_active or None, order=args.serve_order,
-                  adaptive_quantum=args.serve_adaptive)
+                  max_active=args.serve_max_active or None, order=args.serve_order)
         frame_px = [f.width * f.height for f in frames]
         first = clocks is None
         if first:
@@ -848,7 +845,7 @@ def run_serve(args, rank, world, local, dev):
                 "config": {"workload": "serving stream: resolutions {256^2, 512^2, 720p, 1080p, 1440p}, "
                                        "K in {64,128,300}, 40% new 6x64x64 env maps, 60% rotations, "
                                        f"150 GB admission budget, {args.serve_quantum_ms:g} ms quanta, "
-                                       f"order {args.serve_order}{', adaptive quanta' if args.serve_adaptive else ''}",
+                                       f"order {args.serve_order}",
                            "networks": args.serve_nets,
                            "parallelism": f"request-dp{world} with row-band splits" if world > 1 else "1 GPU"},
                 "clocks": clocks, **out}

@@ -4,11 +4,10 @@ Requests of mixed resolution, K and env map arrive over time.  The server keeps 
 network weights and the G-buffers of every resolution resident in HBM, admits requests
 while a device-memory budget allows (their output buffers and env tables), and feeds the
 GPU fixed-size *quanta* of work: each quantum is one ``nwprt_relight_ranges`` launch that
-packs 128-pixel-aligned pixel ranges of several admitted requests, in arrival order
-(``order="fifo"``, the default: it gives the lower p99) or smallest remaining work first
-(``order="srpt"``: lower p50 when the stream overloads the GPU), or earliest deadline first
-(``order="edf"``: a deadline proportional to each request's own size, so that small requests
-are not queued behind large ones).  Requests that arrive while
+packs 128-pixel-aligned pixel ranges of several admitted requests, earliest deadline first
+(``order="edf"``, the default: a deadline proportional to each request's own size, so small
+requests are not queued behind large ones), in arrival order (``order="fifo"``) or smallest
+remaining work first (``order="srpt"``).  Requests that arrive while
 quanta are running join the next quantum, and two quanta are kept in flight so the GPU does
 not idle while the host forms the next one.
 
@@ -249,8 +248,7 @@ class RelightServer:
                  quantum_ms: float = 12.0, est_evals_per_s: float = 9e9, max_queue_s: float = math.inf,
                  max_in_flight: int = 2, keep_outputs: bool = False,
                  fault: Optional[Callable[[Request, str], Optional[str]]] = None,
-                 max_active: Optional[int] = None, order: str = "fifo", completion=None,
-                 adaptive_quantum: bool = False):
+                 max_active: Optional[int] = None, order: str = "edf", completion=None):
         import torch
         self.torch = torch
         self.e = engine
@@ -261,9 +259,6 @@ class RelightServer:
         self.adm = Admission(budget_bytes)
         self.rate = est_evals_per_s
         self.quantum = int(est_evals_per_s * quantum_ms / 1e3)
-        # with adaptive quanta, a request admitted more than one quantum ago and not yet
-        # started shrinks the next quantum (down to a quarter) so that it starts sooner
-        self.adaptive = adaptive_quantum
         self.max_queue_s = max_queue_s
         self.max_in_flight = max_in_flight
         # admission also stops at max_active admitted requests (None: the byte budget alone)
@@ -326,15 +321,6 @@ class RelightServer:
                 except Exception:
                     failed.append(r)
             return failed
-
-    def _quantum_now(self, active: Sequence[Request], t: float) -> int:
-        if not self.adaptive:
-            return self.quantum
-        q_s = self.quantum / self.rate
-        waiting = [t - r.t_admit for r in active if r.next_px == max(0, r.px_lo)]
-        if waiting and max(waiting) > q_s:
-            return max(self.quantum // 4, int(self.quantum * q_s / max(waiting)))
-        return self.quantum
 
     def _retire(self, r: Request, t: float) -> None:
         """A request whose work (and gather) is complete: returns its budget and env table."""
@@ -422,7 +408,7 @@ class RelightServer:
                 active.append(r)
             self.max_active = max(self.max_active, len(active))
             if active and len(in_flight) < self.max_in_flight:
-                plan = plan_quantum(active, self._quantum_now(active, now()), self.order, self.rate)
+                plan = plan_quantum(active, self.quantum, self.order, self.rate)
                 launch = []
                 for r, b, e in plan:
                     try:

@@ -228,13 +228,13 @@ def test_injected_faults_stay_with_their_requests(rig):
             assert torch.equal(r.outputs[0], ind) and torch.equal(r.outputs[1], wd), r.rid
 
 
-@pytest.mark.parametrize("order,adaptive", [("edf", False), ("edf", True), ("srpt", True)])
-def test_packing_orders_keep_results(rig, order, adaptive):
+@pytest.mark.parametrize("order", ["edf", "fifo", "srpt"])
+def test_packing_orders_keep_results(rig, order):
     import torch
     e, frames, base = rig
     reqs = _requests(10, seed=7)
     srv = serve.RelightServer(e, frames, base, precision="bf16", quantum_ms=0.05, est_evals_per_s=9e9,
-                              keep_outputs=True, order=order, adaptive_quantum=adaptive)
+                              keep_outputs=True, order=order)
     stats = srv.run(reqs)
     assert stats["done"] == len(reqs), stats
     for r in reqs:

@@ -109,3 +109,32 @@ def test_validate_request_refuses_malformed_fields():
     for r in bad:
         with pytest.raises(ValueError):
             serve.validate_request(r, n_res=2, face_size=8, n_base=3)
+
+
+def test_edf_packs_small_requests_ahead_of_large_ones():
+    """Earliest deadline first: a deadline of arrival + 4x the request's own service time
+    (at least 16 ms), so a small request that arrives just after a large one goes first."""
+    big = serve.Request(0, 0.000, 0, 300, "new")
+    small = serve.Request(1, 0.001, 0, 64, "new")
+    for r, n in ((big, 2560 * 1440), (small, 256 * 256)):
+        r.n_px, r.next_px = n, 0
+    rate = 5e10
+    assert serve.deadline(small, rate) == pytest.approx(0.001 + 0.016)
+    assert serve.deadline(big, rate) == pytest.approx(4 * 2560 * 1440 * 300 / rate)
+    plan = serve.plan_quantum([big, small], quantum_evals=int(rate * 0.012), order="edf", evals_per_s=rate)
+    assert plan[0][0] is small and plan[0][1:] == (0, 256 * 256)
+    assert plan[1][0] is big and (plan[1][2] - plan[1][1]) % serve.TILE == 0
+    fifo = serve.plan_quantum([big, small], quantum_evals=int(rate * 0.012), order="fifo")
+    assert fifo[0][0] is big
+
+
+def test_class_latency_splits_at_720p():
+    frames = [256 * 256, 1280 * 720, 1920 * 1080]
+    reqs = []
+    for i, (res, lat) in enumerate([(0, 0.004), (1, 0.010), (2, 0.030), (2, 0.050)]):
+        r = serve.Request(i, 0.0, res, 64, "new")
+        r.status, r.t_done = "done", lat
+        reqs.append(r)
+    c = serve.class_latency(reqs, frames)
+    assert c["small"]["done"] == 2 and c["large"]["done"] == 2
+    assert c["small"]["p50_ms"] == pytest.approx(7.0) and c["large"]["p50_ms"] == pytest.approx(40.0)
