@@ -2,7 +2,8 @@
 
 The reference ships no tests or golden data for this path; the oracle is pinned here by
 (1) analytic known answers, (2) an independent numpy restatement, (3) the reference's
-own utils_kernels.h compiled for the host (oracle/_ref), and (4) committed fixtures.
+own utils_kernels.h compiled for the host (oracle/_ref), and (4) the committed fixtures of
+tests/golden/ (checked in tests/test_golden.py).
 """
 import math
 
