@@ -354,7 +354,9 @@ class RelightServer:
         now = lambda: time.perf_counter() - t0
         finished = 0
         total = len(requests)
-        while finished < total:
+        # transfers of refused or failed bands may still be queued once every request has
+        # ended here: the loop runs until the completion has nothing outstanding either
+        while finished < total or self.completion.outstanding():
             for r in self.completion.poll():
                 gathering.remove(r)
                 self._retire(r, now())

@@ -80,8 +80,11 @@ def _worker(rank, world, port, faults, q):
         fault = None
         if rank in faults:
             def fault(r, stage, mine=tuple(faults[rank])):
+                if ("drop", r.rid) in mine and stage == "arrive":
+                    return "drop"
                 if (stage, r.rid) in mine:
                     raise RuntimeError("injected")
+                return None
         dist.barrier()
         summ = dispatch.serve_distributed(
             FakeEngine(), frames, [], reqs, rank, world, channels, "cpu", evals_per_s=1e6, split_min_evals=SPLIT_MIN,
@@ -179,11 +182,14 @@ def test_injected_failures_end_only_their_requests():
     # split request, fails its own part at admission
     rid_band = next(rid for rid in split if plan[rid][0] == 0)
     rid_owner = next(rid for rid in split if plan[rid][0] == 1)
-    out = _run({1: [("launch", rid_band), ("admit", rid_owner)]})
+    # rank 0 loses its band of the earliest split request rank 1 owns (dropped in transit):
+    # the band still goes out, flagged, ahead of rank 0's later bands for rank 1
+    rid_drop = next(rid for rid in split if plan[rid][0] == 1 and rid != rid_owner)
+    out = _run({1: [("launch", rid_band), ("admit", rid_owner)], 0: [("drop", rid_drop)]})
     owned = {}
     for o, bad, _, _ in out:
         assert not bad
         owned.update(o)
     assert sorted(owned) == list(range(40))
     not_done = sorted(rid for rid, st in owned.items() if st != "done")
-    assert not_done == sorted([rid_band, rid_owner]), not_done
+    assert not_done == sorted([rid_band, rid_owner, rid_drop]), not_done
