@@ -566,6 +566,13 @@ __global__ void __launch_bounds__(kThreads, 2)
     // ---- the six transforms: keys to shared memory, coefficients to the scratch slice
     for (int f = 0; f < 6; ++f) {
       const float* src = faces + ((size_t)env * 6 + f) * (size_t)SS * 3;
+      // the next face (after the sixth: this CTA's next map's first) into L2 meanwhile
+      if (tid == 0 && (SS * 12) % 16 == 0) {
+        const long long nxt = (long long)env * 6 + f + 1 + (f == 5 ? (long long)(gridDim.x - 1) * 6 : 0);
+        const float* pf = faces + (size_t)nxt * SS * 3;
+        if (nxt < (long long)n_env * 6 && (reinterpret_cast<uintptr_t>(pf) & 15) == 0)
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(pf), "r"((uint32_t)(SS * 12)) : "memory");
+      }
       float co[NR > 0 ? NR : 1][3];
       haar_face_in_registers<S>(src, tid, co, sm.upper, sm.llg);
       uint32_t k[NKQ * 4];
@@ -589,11 +596,73 @@ __global__ void __launch_bounds__(kThreads, 2)
         sm.keys[((size_t)f * NKQ + q) * kThreads + tid] = make_uint4(k[4 * q], k[4 * q + 1], k[4 * q + 2], k[4 * q + 3]);
       __syncthreads();  // the next face reuses `upper`
     }
-    // ---- 4-pass radix select of the K-th largest key
+    // ---- radix select of the K-th largest key.  The keys' top bits are mostly exponent, so a
+    // plain first pass piles 24K keys into a few bins (serialised shared atomics).  Instead the
+    // first pass histograms only keys within 16 binades of the largest key, at 1/16 binade
+    // (256 bins on bits 30..19; keys are non-negative, bit 31 is 0).  If that window holds K
+    // keys or more, the K-th largest is in it and the remaining 19 bits take passes of 8, 8
+    // and 3 bits over the few keys that match the prefix; otherwise four 8-bit passes.
     uint32_t prefix = 0, mask = 0;
     int remaining = K;
-    for (int pass = 0; pass < 4; ++pass) {
-      const int shift = 24 - 8 * pass;
+    int shifts[4] = {24, 16, 8, 0}, widths[4] = {8, 8, 8, 8}, n_pass = 4;
+    {
+      uint32_t kmax = 0;
+      if (owner)
+        for (int f = 0; f < 6; ++f)
+#pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            kmax = max(max(kmax, max(v.x, v.y)), max(v.z, v.w));
+          }
+      kmax = __reduce_max_sync(0xffffffffu, kmax);
+      if (lane == 0) sm.warp_tot[warp] = (int)kmax;
+      for (int i = tid; i < kWarps * 256; i += kThreads) sm.whist[i] = 0u;
+      __syncthreads();
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) kmax = max(kmax, (uint32_t)sm.warp_tot[w]);
+      const int e_lo = (int)(kmax >> 23) - 15;
+      if (owner) {
+        uint32_t* h = sm.whist + warp * 256;
+        for (int f = 0; f < 6; ++f)
+#pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const int e = (int)(kk[i] >> 23);
+              if (4 * q + i < NK && e >= e_lo) atomicAdd(&h[((e - e_lo) << 4) | ((kk[i] >> 19) & 15u)], 1u);
+            }
+          }
+      }
+      __syncthreads();
+      const int bin = 255 - tid;
+      uint32_t tot = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) tot += sm.whist[w * 256 + bin];
+      uint32_t all;
+      const uint32_t incl = block_inclusive_sum(tot, sm.warp_tot, &all);  // its barriers order the reads above
+      if (tid == 0) sm.scal[kScRemaining] = -1;  // stays -1 when the window holds fewer than K keys
+      __syncthreads();
+      if (incl >= (uint32_t)K && incl - tot < (uint32_t)K) {
+        sm.scal[kScPrefix] = (int)((uint32_t)(((e_lo + (bin >> 4)) << 4) | (bin & 15)) << 19);
+        sm.scal[kScRemaining] = K - (int)(incl - tot);
+      }
+      __syncthreads();
+      if (sm.scal[kScRemaining] >= 0) {
+        prefix = (uint32_t)sm.scal[kScPrefix];
+        mask = 0xFFF80000u;
+        remaining = sm.scal[kScRemaining];
+        shifts[0] = 11;
+        shifts[1] = 3;
+        shifts[2] = 0;
+        widths[2] = 3;
+        n_pass = 3;
+      }
+    }
+    for (int pass = 0; pass < n_pass; ++pass) {
+      const int shift = shifts[pass];
+      const uint32_t dmask = (1u << widths[pass]) - 1u;
       for (int i = tid; i < kWarps * 256; i += kThreads) sm.whist[i] = 0u;
       __syncthreads();
       if (owner) {
@@ -605,11 +674,11 @@ __global__ void __launch_bounds__(kThreads, 2)
             const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (int i = 0; i < 4; ++i)
-              if (4 * q + i < NK && (kk[i] & mask) == prefix) atomicAdd(&h[(kk[i] >> shift) & 255u], 1u);
+              if (4 * q + i < NK && (kk[i] & mask) == prefix) atomicAdd(&h[(kk[i] >> shift) & dmask], 1u);
           }
       }
       __syncthreads();
-      const int digit = 255 - tid;
+      const int digit = 255 - tid;  // digits above dmask hold no keys
       uint32_t tot = 0;
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) tot += sm.whist[w * 256 + digit];
@@ -617,7 +686,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       const uint32_t incl = block_inclusive_sum(tot, sm.warp_tot, &all);
       if (incl >= (uint32_t)remaining && incl - tot < (uint32_t)remaining) {
         sm.scal[kScPrefix] = (int)(prefix | ((uint32_t)digit << shift));
-        sm.scal[kScMask] = (int)(mask | (255u << shift));
+        sm.scal[kScMask] = (int)(mask | (dmask << shift));
         sm.scal[kScRemaining] = remaining - (int)(incl - tot);
       }
       __syncthreads();
