@@ -64,6 +64,10 @@ struct HaarSmem {
 
 // scal[] slots
 constexpr int kScPrefix = 0, kScMask = 1, kScRemaining = 2, kScCounter = 3, kScEq = 8;  // eq: [6]
+constexpr int kScNAbove = 16, kScNCand = 17;  // batched kernel: winners above the window bin, candidates in it
+// Candidates (keys in the window's selected bin) the batched kernel ranks directly; they share
+// the histogram region: composite keys (8 B) + ids (4 B).
+constexpr int kCandCap = 680;
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -112,6 +116,18 @@ __device__ __forceinline__ uint32_t wavelet_key_bits(float r, float g, float b) 
   t = fabsf(t);
   if (t != t) t = 0.0f;
   return __float_as_uint(t);
+}
+
+// A face texel vector read once: marked first to leave L2, so the input stream does not evict
+// the batched kernel's coefficient scratch.
+__device__ __forceinline__ float4 ld_stream_f4(const float4* p) {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  float4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p), "l"(pol));
+  return v;
 }
 
 // Bits 0, 2, 4, 6 of x packed into bits 0..3 (Morton decode of one coordinate).
@@ -229,7 +245,7 @@ __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__
           const float4* row = reinterpret_cast<const float4*>(blk + (size_t)r * S * 3);
 #pragma unroll
           for (int q = 0; q < 3; ++q) {
-            const float4 v = __ldg(row + q);
+            const float4 v = ld_stream_f4(row + q);
             const float e[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (int k = 0; k < 4; ++k) px[r][(4 * q + k) / 3][(4 * q + k) % 3] = e[k];
@@ -660,128 +676,206 @@ __global__ void __launch_bounds__(kThreads, 2)
         n_pass = 3;
       }
     }
-    for (int pass = 0; pass < n_pass; ++pass) {
-      const int shift = shifts[pass];
-      const uint32_t dmask = (1u << widths[pass]) - 1u;
-      for (int i = tid; i < kWarps * 256; i += kThreads) sm.whist[i] = 0u;
+    // ---- the window's bin was found: every key above it wins, the keys in it are candidates.
+    // One scan sorts them (warp-aggregated slots); the candidates, usually a few dozen, are
+    // ranked among themselves.  More candidates than fit: the general passes below.
+    bool fast = false;
+    if (n_pass == 3) {
+      if (tid == 0) {
+        sm.scal[kScNAbove] = 0;
+        sm.scal[kScNCand] = 0;
+      }
       __syncthreads();
-      if (owner) {
-        uint32_t* h = sm.whist + warp * 256;
+      uint64_t* ckey = reinterpret_cast<uint64_t*>(sm.whist);
+      int* cid = reinterpret_cast<int*>(ckey + kCandCap);
+      const uint32_t P = prefix >> 19;
+      const uint32_t lt = (1u << lane) - 1u;
+      if (owner || warp * 32 < T)  // whole warps take part in the ballots
         for (int f = 0; f < 6; ++f)
 #pragma unroll
           for (int q = 0; q < NKQ; ++q) {
             const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
             const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const int u = 4 * q + i;
+              const bool live = owner && u < NK;
+              const bool win = live && (kk[i] >> 19) > P;
+              const bool cand = live && (kk[i] >> 19) == P;
+              const unsigned mw = __ballot_sync(0xffffffffu, win), mc = __ballot_sync(0xffffffffu, cand);
+              if (!(mw | mc)) continue;
+              int bw = 0, bc = 0;
+              if (lane == 0) {
+                if (mw) bw = atomicAdd(&sm.scal[kScNAbove], __popc(mw));
+                if (mc) bc = atomicAdd(&sm.scal[kScNCand], __popc(mc));
+              }
+              bw = __shfl_sync(0xffffffffu, bw, 0);
+              bc = __shfl_sync(0xffffffffu, bc, 0);
+              if (win || cand) {
+                const int g = f * SS + flat_in_face<S>(tid, u);
+                const uint64_t ck = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
+                const int id = (f * NK + u) * kThreads + tid;
+                if (win) {
+                  const int slot = bw + __popc(mw & lt);
+                  sm.gkey[slot] = ck;
+                  sm.gid[slot] = id;
+                } else {
+                  const int c = bc + __popc(mc & lt);
+                  if (c < kCandCap) {
+                    ckey[c] = ck;
+                    cid[c] = id;
+                  }
+                }
+              }
+            }
+          }
+      __syncthreads();
+      const int n_cand = sm.scal[kScNCand];
+      if (n_cand <= kCandCap) {
+        fast = true;
+        const int n_above = sm.scal[kScNAbove];  // == K - remaining
+        for (int c = tid; c < n_cand; c += kThreads) {
+          const uint64_t me = ckey[c];
+          int rank = 0;
+          for (int o = 0; o < n_cand; ++o) rank += ckey[o] > me;
+          if (rank < remaining) {
+            sm.gkey[n_above + rank] = me;
+            sm.gid[n_above + rank] = cid[c];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (!fast) {
+      for (int pass = 0; pass < n_pass; ++pass) {
+        const int shift = shifts[pass];
+        const uint32_t dmask = (1u << widths[pass]) - 1u;
+        for (int i = tid; i < kWarps * 256; i += kThreads) sm.whist[i] = 0u;
+        __syncthreads();
+        if (owner) {
+          uint32_t* h = sm.whist + warp * 256;
+          for (int f = 0; f < 6; ++f)
+  #pragma unroll
+            for (int q = 0; q < NKQ; ++q) {
+              const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+              const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+  #pragma unroll
+              for (int i = 0; i < 4; ++i)
+                if (4 * q + i < NK && (kk[i] & mask) == prefix) atomicAdd(&h[(kk[i] >> shift) & dmask], 1u);
+            }
+        }
+        __syncthreads();
+        const int digit = 255 - tid;  // digits above dmask hold no keys
+        uint32_t tot = 0;
+  #pragma unroll
+        for (int w = 0; w < kWarps; ++w) tot += sm.whist[w * 256 + digit];
+        uint32_t all;
+        const uint32_t incl = block_inclusive_sum(tot, sm.warp_tot, &all);
+        if (incl >= (uint32_t)remaining && incl - tot < (uint32_t)remaining) {
+          sm.scal[kScPrefix] = (int)(prefix | ((uint32_t)digit << shift));
+          sm.scal[kScMask] = (int)(mask | (dmask << shift));
+          sm.scal[kScRemaining] = remaining - (int)(incl - tot);
+        }
+        __syncthreads();
+        prefix = (uint32_t)sm.scal[kScPrefix];
+        mask = (uint32_t)sm.scal[kScMask];
+        remaining = sm.scal[kScRemaining];
+      }
+      // ---- ties at the threshold in flat-index order: a bitmap over face * S*S + flat
+      const uint32_t thr = prefix;
+      for (int w = tid; w < NW; w += kThreads) sm.bits[w] = 0u;
+      __syncthreads();
+      if (owner)
+        for (int f = 0; f < 6; ++f)
+  #pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+  #pragma unroll
             for (int i = 0; i < 4; ++i)
-              if (4 * q + i < NK && (kk[i] & mask) == prefix) atomicAdd(&h[(kk[i] >> shift) & dmask], 1u);
+              if (4 * q + i < NK && kk[i] == thr) {
+                const int g = f * SS + flat_in_face<S>(tid, 4 * q + i);
+                atomicOr(&sm.bits[g >> 5], 1u << (g & 31));
+              }
           }
+      __syncthreads();
+      {
+        // exclusive popcount prefix over the bitmap: thread t covers words [t*per, t*per + per)
+        constexpr int PER = (NW + kThreads - 1) / kThreads;
+        uint32_t pc[PER], mine = 0;
+  #pragma unroll
+        for (int i = 0; i < PER; ++i) {
+          const int w = tid * PER + i;
+          pc[i] = w < NW ? (uint32_t)__popc(sm.bits[w]) : 0u;
+          mine += pc[i];
+        }
+        uint32_t all;
+        uint32_t run = block_inclusive_sum(mine, sm.warp_tot, &all) - mine;
+  #pragma unroll
+        for (int i = 0; i < PER; ++i) {
+          const int w = tid * PER + i;
+          if (w < NW) sm.wpre[w] = run;
+          run += pc[i];
+        }
       }
       __syncthreads();
-      const int digit = 255 - tid;  // digits above dmask hold no keys
-      uint32_t tot = 0;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) tot += sm.whist[w * 256 + digit];
-      uint32_t all;
-      const uint32_t incl = block_inclusive_sum(tot, sm.warp_tot, &all);
-      if (incl >= (uint32_t)remaining && incl - tot < (uint32_t)remaining) {
-        sm.scal[kScPrefix] = (int)(prefix | ((uint32_t)digit << shift));
-        sm.scal[kScMask] = (int)(mask | (dmask << shift));
-        sm.scal[kScRemaining] = remaining - (int)(incl - tot);
-      }
+      // ---- winners: slots from one block scan of per-thread counts
+      int n_sel = 0;
+      if (owner)
+        for (int f = 0; f < 6; ++f)
+  #pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+  #pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              if (4 * q + i >= NK) continue;
+              bool sel = kk[i] > thr;
+              if (kk[i] == thr) {
+                const int g = f * SS + flat_in_face<S>(tid, 4 * q + i), w = g >> 5;
+                sel = (int)(sm.wpre[w] + __popc(sm.bits[w] & ((1u << (g & 31)) - 1u))) < remaining;
+              }
+              n_sel += sel;
+            }
+          }
+      uint32_t all_sel;
+      int slot = (int)block_inclusive_sum((uint32_t)n_sel, sm.warp_tot, &all_sel) - n_sel;
+      if (owner && n_sel)
+        for (int f = 0; f < 6; ++f)
+  #pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+  #pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              if (4 * q + i >= NK) continue;
+              const int u = 4 * q + i;
+              const int g = f * SS + flat_in_face<S>(tid, u);
+              bool sel = kk[i] > thr;
+              if (kk[i] == thr) {
+                const int w = g >> 5;
+                sel = (int)(sm.wpre[w] + __popc(sm.bits[w] & ((1u << (g & 31)) - 1u))) < remaining;
+              }
+              if (sel) {
+                sm.gkey[slot] = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
+                sm.gid[slot] = (f * NK + u) * kThreads + tid;
+                ++slot;
+              }
+            }
+          }
       __syncthreads();
-      prefix = (uint32_t)sm.scal[kScPrefix];
-      mask = (uint32_t)sm.scal[kScMask];
-      remaining = sm.scal[kScRemaining];
     }
-    // ---- ties at the threshold in flat-index order: a bitmap over face * S*S + flat
-    const uint32_t thr = prefix;
-    for (int w = tid; w < NW; w += kThreads) sm.bits[w] = 0u;
-    __syncthreads();
-    if (owner)
-      for (int f = 0; f < 6; ++f)
-#pragma unroll
-        for (int q = 0; q < NKQ; ++q) {
-          const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
-          const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (4 * q + i < NK && kk[i] == thr) {
-              const int g = f * SS + flat_in_face<S>(tid, 4 * q + i);
-              atomicOr(&sm.bits[g >> 5], 1u << (g & 31));
-            }
-        }
-    __syncthreads();
-    {
-      // exclusive popcount prefix over the bitmap: thread t covers words [t*per, t*per + per)
-      constexpr int PER = (NW + kThreads - 1) / kThreads;
-      uint32_t pc[PER], mine = 0;
-#pragma unroll
-      for (int i = 0; i < PER; ++i) {
-        const int w = tid * PER + i;
-        pc[i] = w < NW ? (uint32_t)__popc(sm.bits[w]) : 0u;
-        mine += pc[i];
-      }
-      uint32_t all;
-      uint32_t run = block_inclusive_sum(mine, sm.warp_tot, &all) - mine;
-#pragma unroll
-      for (int i = 0; i < PER; ++i) {
-        const int w = tid * PER + i;
-        if (w < NW) sm.wpre[w] = run;
-        run += pc[i];
-      }
-    }
-    __syncthreads();
-    // ---- winners: slots from one block scan of per-thread counts
-    int n_sel = 0;
-    if (owner)
-      for (int f = 0; f < 6; ++f)
-#pragma unroll
-        for (int q = 0; q < NKQ; ++q) {
-          const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
-          const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            if (4 * q + i >= NK) continue;
-            bool sel = kk[i] > thr;
-            if (kk[i] == thr) {
-              const int g = f * SS + flat_in_face<S>(tid, 4 * q + i), w = g >> 5;
-              sel = (int)(sm.wpre[w] + __popc(sm.bits[w] & ((1u << (g & 31)) - 1u))) < remaining;
-            }
-            n_sel += sel;
-          }
-        }
-    uint32_t all_sel;
-    int slot = (int)block_inclusive_sum((uint32_t)n_sel, sm.warp_tot, &all_sel) - n_sel;
-    if (owner && n_sel)
-      for (int f = 0; f < 6; ++f)
-#pragma unroll
-        for (int q = 0; q < NKQ; ++q) {
-          const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
-          const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            if (4 * q + i >= NK) continue;
-            const int u = 4 * q + i;
-            const int g = f * SS + flat_in_face<S>(tid, u);
-            bool sel = kk[i] > thr;
-            if (kk[i] == thr) {
-              const int w = g >> 5;
-              sel = (int)(sm.wpre[w] + __popc(sm.bits[w] & ((1u << (g & 31)) - 1u))) < remaining;
-            }
-            if (sel) {
-              sm.gkey[slot] = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
-              sm.gid[slot] = (f * NK + u) * kThreads + tid;
-              ++slot;
-            }
-          }
-        }
-    __syncthreads();
     // ---- rank the K winners (broadcast reads of the composite keys) and write them out
     for (int e = tid; e < K; e += kThreads) {
       const uint64_t me = sm.gkey[e];
-      int rank = 0;
-      for (int o = 0; o < K; ++o) rank += sm.gkey[o] > me;
+      int rank = 0, o = 0;
+      for (; o + 8 <= K; o += 8) {  // eight broadcast loads in flight
+        int r = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r += sm.gkey[o + j] > me;
+        rank += r;
+      }
+      for (; o < K; ++o) rank += sm.gkey[o] > me;
       const int id = sm.gid[e];
       const int t = id % kThreads, fu = id / kThreads, f = fu / NK, u = fu % NK;
       const size_t out = (size_t)env * K + rank;
