@@ -118,18 +118,6 @@ __device__ __forceinline__ uint32_t wavelet_key_bits(float r, float g, float b) 
   return __float_as_uint(t);
 }
 
-// A face texel vector read once: marked first to leave L2, so the input stream does not evict
-// the batched kernel's coefficient scratch.
-__device__ __forceinline__ float4 ld_stream_f4(const float4* p) {
-  uint64_t pol;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  float4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "l"(p), "l"(pol));
-  return v;
-}
-
 // Bits 0, 2, 4, 6 of x packed into bits 0..3 (Morton decode of one coordinate).
 __device__ __forceinline__ int morton_even(int x) {
   x &= 0x55;
@@ -245,7 +233,7 @@ __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__
           const float4* row = reinterpret_cast<const float4*>(blk + (size_t)r * S * 3);
 #pragma unroll
           for (int q = 0; q < 3; ++q) {
-            const float4 v = ld_stream_f4(row + q);
+            const float4 v = __ldg(row + q);
             const float e[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (int k = 0; k < 4; ++k) px[r][(4 * q + k) / 3][(4 * q + k) % 3] = e[k];
