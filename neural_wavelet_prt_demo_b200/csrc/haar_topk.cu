@@ -126,7 +126,9 @@ __device__ __forceinline__ int morton_even(int x) {
   return x;
 }
 
-// Inclusive prefix of `v` over the block's threads in thread order; `total` = block sum.
+// Inclusive prefix of `v` over the block's threads in thread order (a block of NWARPS warps);
+// `total` = block sum.
+template <int NWARPS = kWarps>
 __device__ __forceinline__ uint32_t block_inclusive_sum(uint32_t v, int* warp_tot, uint32_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t incl = v;
@@ -139,7 +141,7 @@ __device__ __forceinline__ uint32_t block_inclusive_sum(uint32_t v, int* warp_to
   __syncthreads();
   uint32_t before = 0, all = 0;
 #pragma unroll
-  for (int w = 0; w < kWarps; ++w) {
+  for (int w = 0; w < NWARPS; ++w) {
     const uint32_t t = (uint32_t)warp_tot[w];
     before += (w < warp) ? t : 0u;
     all += t;
@@ -203,6 +205,35 @@ __device__ __forceinline__ int flat_in_face(int tid, int u) {
   }
   const int band = u % 3;
   return band == 0 ? i * S + j + h : (band == 1 ? (i + h) * S + j : (i + h) * S + j + h);
+}
+
+// Coefficient u < NR of thread tid's texel block (all three channels), recomputed from the
+// face at `src` with the same FP32 operations, in the same order, as the transform below:
+// a level-1 detail from its 2x2 quad, a level-2 detail from the four quads' LL values.  The
+// batched kernel keeps no copy of these coefficients; it recomputes the K winners' instead.
+template <int S>
+__device__ __forceinline__ void block_coef(const float* __restrict__ src, int tid, int u, float (&out)[3]) {
+  using F = FaceGeom<S>;
+  const int bj = morton_even(tid), bi = morton_even(tid >> 1);
+  const float* blk = src + ((size_t)(F::B * bi) * S + F::B * bj) * 3;
+  const int q = u / 3, band = u % 3;
+  auto quad = [&](int qi, int qj, int c, float& a, float& hl, float& lh, float& hh) {
+    const float* p0 = blk + ((size_t)(2 * qi) * S + 2 * qj) * 3 + c;
+    haar4(__ldg(p0), __ldg(p0 + 3), __ldg(p0 + S * 3), __ldg(p0 + S * 3 + 3), a, hl, lh, hh);
+  };
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float a, hl, lh, hh;
+    if (q < 4) {
+      quad(q >> 1, q & 1, c, a, hl, lh, hh);
+    } else {
+      float l1[4], x, y, z;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) quad(k >> 1, k & 1, c, l1[k], x, y, z);
+      haar4(l1[0], l1[1], l1[2], l1[3], a, hl, lh, hh);
+    }
+    out[c] = band == 0 ? hl : (band == 1 ? lh : hh);
+  }
 }
 
 // The full Haar transform of one face [S][S][3] at `src` by the block's kThreads threads:
@@ -493,11 +524,13 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
 // One persistent CTA per map at a time (no cluster): for large batches, whole maps in flight
 // per SM beat the cluster's one sixth of a map each, and no step crosses an SM.  Faces are
 // transformed one after another with the same register code; the keys of all six stay in
-// shared memory (uint4 of four keys, thread-fastest: conflict-free), the coefficients go to
-// this CTA's slice of a global scratch buffer ([face][u][channel][thread], coalesced; it
-// stays in L2 because every CTA reuses its own slice map after map).  The select is the
-// cluster form's, block-local: per-warp histograms, a bitmap of ties over the 6*S*S flat
-// indices, winner slots from one block scan, and a rank by broadcast reads of the K keys.
+// shared memory (uint4 of four keys, thread-fastest: conflict-free).  Of the coefficients
+// only each thread's upper-block entry is kept, in this CTA's slice of a global scratch
+// buffer ([face][channel][thread], 18 KB at S = 64, so it stays in L2); the K winners' other
+// coefficients are recomputed from their texel blocks (block_coef), which costs far less
+// than writing and re-reading all 6 * S * S of them.  The select is the cluster form's,
+// block-local: per-warp histograms, a bitmap of ties over the 6*S*S flat indices, winner
+// slots from one block scan, and a rank by broadcast reads of the K keys.
 
 struct BatchSmem {
   uint4* keys;      // [6][NK/4][kThreads]
@@ -544,8 +577,8 @@ __host__ __device__ inline size_t batch_smem_layout(int S, int K, char* base, Ba
 }
 
 template <int S>
-constexpr size_t batch_scratch_floats_per_cta() {
-  return (size_t)6 * FaceGeom<S>::NK * 3 * kThreads;
+__host__ __device__ constexpr size_t batch_scratch_floats_per_cta() {
+  return (size_t)6 * 3 * kThreads;
 }
 
 template <int S>
@@ -557,17 +590,21 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr int NKQ = (NK + 3) / 4;
   constexpr int NW = (6 * SS + 31) / 32;
   static_assert(T <= kThreads, "one 4x4 block per thread");
+  static_assert(kThreads == 256, "one thread per bin of the winners' counting pass");
+  static_assert(512 * sizeof(uint32_t) + kMaxK * sizeof(uint16_t) <= kWarps * 256 * sizeof(uint32_t),
+                "the winners' bins and order fit the histogram region");
   extern __shared__ __align__(16) char smem_raw[];
   BatchSmem sm;
   batch_smem_layout(S, K, smem_raw, &sm);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool owner = tid < T;
-  float* rgb = scratch + (size_t)blockIdx.x * batch_scratch_floats_per_cta<S>();
-  // [face][u][channel][thread]
-  auto rgb_at = [&](int f, int u, int c, int t) -> float* { return rgb + (((size_t)f * NK + u) * 3 + c) * kThreads + t; };
+  // this CTA's upper-block entries, [face][channel][thread]
+  float* up = scratch + (size_t)blockIdx.x * batch_scratch_floats_per_cta<S>();
 
   for (int env = blockIdx.x; env < n_env; env += gridDim.x) {
-    // ---- the six transforms: keys to shared memory, coefficients to the scratch slice
+    // ---- the six transforms: keys to shared memory, upper-block entries to the scratch slice;
+    // each thread keeps the largest key it formed
+    uint32_t kmax = 0;
     for (int f = 0; f < 6; ++f) {
       const float* src = faces + ((size_t)env * 6 + f) * (size_t)SS * 3;
       // the next face (after the sixth: this CTA's next map's first) into L2 meanwhile
@@ -584,16 +621,14 @@ __global__ void __launch_bounds__(kThreads, 2)
       for (int u = 0; u < NKQ * 4; ++u) k[u] = 0u;
       if (owner) {
 #pragma unroll
-        for (int u = 0; u < NR; ++u) {
-          k[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) *rgb_at(f, u, c, tid) = co[u][c];
-        }
+        for (int u = 0; u < NR; ++u) k[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
         const float ur = sm.upper[tid * 3], ug = sm.upper[tid * 3 + 1], ub = sm.upper[tid * 3 + 2];
         k[NR] = wavelet_key_bits(ur, ug, ub);
-        *rgb_at(f, NR, 0, tid) = ur;
-        *rgb_at(f, NR, 1, tid) = ug;
-        *rgb_at(f, NR, 2, tid) = ub;
+#pragma unroll
+        for (int u = 0; u <= NR; ++u) kmax = max(kmax, k[u]);
+        up[(f * 3 + 0) * kThreads + tid] = ur;
+        up[(f * 3 + 1) * kThreads + tid] = ug;
+        up[(f * 3 + 2) * kThreads + tid] = ub;
       }
 #pragma unroll
       for (int q = 0; q < NKQ; ++q)
@@ -610,15 +645,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     int remaining = K;
     int shifts[4] = {24, 16, 8, 0}, widths[4] = {8, 8, 8, 8}, n_pass = 4;
     {
-      uint32_t kmax = 0;
-      if (owner)
-        for (int f = 0; f < 6; ++f)
-#pragma unroll
-          for (int q = 0; q < NKQ; ++q) {
-            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
-            kmax = max(max(kmax, max(v.x, v.y)), max(v.z, v.w));
-          }
-      kmax = __reduce_max_sync(0xffffffffu, kmax);
+      kmax = __reduce_max_sync(0xffffffffu, kmax);  // then over the block: the map's largest key
       if (lane == 0) sm.warp_tot[warp] = (int)kmax;
       for (int i = tid; i < kWarps * 256; i += kThreads) sm.whist[i] = 0u;
       __syncthreads();
@@ -853,24 +880,47 @@ __global__ void __launch_bounds__(kThreads, 2)
           }
       __syncthreads();
     }
-    // ---- rank the K winners (broadcast reads of the composite keys) and write them out
+    // ---- order the K winners.  Every winner's key lies in [prefix, kmax] (prefix: the window
+    // bin's lower edge or the exact threshold), so a counting pass over 256 bins of that range
+    // (bin 0 = the largest keys) places them, and each is ranked only among the few winners of
+    // its own bin by the composite key.  The histogram region is free again here.
+    uint32_t* bin_n = sm.whist;                                    // [256] winners per bin
+    uint32_t* bin_end = sm.whist + 256;                            // [256] scatter cursor
+    uint16_t* order = reinterpret_cast<uint16_t*>(sm.whist + 512);  // [K] winners by bin
+    const uint32_t range = kmax - prefix;
+    const int bshift = range < 256u ? 0 : 24 - __clz((int)range);  // (range >> bshift) < 256
+    auto bin_of = [&](uint64_t ck) { return (kmax - (uint32_t)(ck >> 32)) >> bshift; };
+    bin_n[tid] = 0u;  // kThreads == 256 bins
+    __syncthreads();
+    for (int e = tid; e < K; e += kThreads) atomicAdd(&bin_n[bin_of(sm.gkey[e])], 1u);
+    __syncthreads();
+    {
+      uint32_t all;
+      const uint32_t n = bin_n[tid];
+      bin_end[tid] = block_inclusive_sum(n, sm.warp_tot, &all) - n;  // starts; ends after the scatter
+    }
+    __syncthreads();
+    for (int e = tid; e < K; e += kThreads) order[atomicAdd(&bin_end[bin_of(sm.gkey[e])], 1u)] = (uint16_t)e;
+    __syncthreads();
     for (int e = tid; e < K; e += kThreads) {
       const uint64_t me = sm.gkey[e];
-      int rank = 0, o = 0;
-      for (; o + 8 <= K; o += 8) {  // eight broadcast loads in flight
-        int r = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) r += sm.gkey[o + j] > me;
-        rank += r;
-      }
-      for (; o < K; ++o) rank += sm.gkey[o] > me;
+      const uint32_t b = bin_of(me), end = bin_end[b];
+      int rank = (int)(end - bin_n[b]);
+      for (uint32_t i = end - bin_n[b]; i < end; ++i) rank += sm.gkey[order[i]] > me;
       const int id = sm.gid[e];
       const int t = id % kThreads, fu = id / kThreads, f = fu / NK, u = fu % NK;
       const size_t out = (size_t)env * K + rank;
+      float v[3] = {0.f, 0.f, 0.f};
+      if (u == NR) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = up[(f * 3 + c) * kThreads + t];
+      } else if constexpr (NR > 0) {
+        block_coef<S>(faces + ((size_t)env * 6 + f) * (size_t)SS * 3, t, u, v);
+      }
       idx_out[out] = f * SS + flat_in_face<S>(t, u);
-      st_out[out * 3 + 0] = *rgb_at(f, u, 0, t);
-      st_out[out * 3 + 1] = *rgb_at(f, u, 1, t);
-      st_out[out * 3 + 2] = *rgb_at(f, u, 2, t);
+      st_out[out * 3 + 0] = v[0];
+      st_out[out * 3 + 1] = v[1];
+      st_out[out * 3 + 2] = v[2];
     }
     __syncthreads();  // the next map reuses every shared array and the scratch slice
   }
