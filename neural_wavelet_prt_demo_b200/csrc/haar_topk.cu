@@ -692,8 +692,10 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     }
     // ---- the window's bin was found: every key above it wins, the keys in it are candidates.
-    // One scan sorts them (warp-aggregated slots); the candidates, usually a few dozen, are
-    // ranked among themselves.  More candidates than fit: the general passes below.
+    // One scan sorts them: a group of four keys below the bin (almost all of them) costs one
+    // compare, and each of the ~1% that reach it takes a slot with a shared atomic.  The
+    // candidates, usually a few dozen, are ranked among themselves.  More candidates than fit:
+    // the general passes below.
     bool fast = false;
     if (n_pass == 3) {
       if (tid == 0) {
@@ -703,43 +705,30 @@ __global__ void __launch_bounds__(kThreads, 2)
       __syncthreads();
       uint64_t* ckey = reinterpret_cast<uint64_t*>(sm.whist);
       int* cid = reinterpret_cast<int*>(ckey + kCandCap);
-      const uint32_t P = prefix >> 19;
-      const uint32_t lt = (1u << lane) - 1u;
-      if (owner || warp * 32 < T)  // whole warps take part in the ballots
+      const uint32_t lo_key = prefix, hi_key = prefix + (1u << 19);  // the bin is [lo_key, hi_key)
+      if (owner)
         for (int f = 0; f < 6; ++f)
 #pragma unroll
           for (int q = 0; q < NKQ; ++q) {
             const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            if (max(max(v.x, v.y), max(v.z, v.w)) < lo_key) continue;
             const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
               const int u = 4 * q + i;
-              const bool live = owner && u < NK;
-              const bool win = live && (kk[i] >> 19) > P;
-              const bool cand = live && (kk[i] >> 19) == P;
-              const unsigned mw = __ballot_sync(0xffffffffu, win), mc = __ballot_sync(0xffffffffu, cand);
-              if (!(mw | mc)) continue;
-              int bw = 0, bc = 0;
-              if (lane == 0) {
-                if (mw) bw = atomicAdd(&sm.scal[kScNAbove], __popc(mw));
-                if (mc) bc = atomicAdd(&sm.scal[kScNCand], __popc(mc));
-              }
-              bw = __shfl_sync(0xffffffffu, bw, 0);
-              bc = __shfl_sync(0xffffffffu, bc, 0);
-              if (win || cand) {
-                const int g = f * SS + flat_in_face<S>(tid, u);
-                const uint64_t ck = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
-                const int id = (f * NK + u) * kThreads + tid;
-                if (win) {
-                  const int slot = bw + __popc(mw & lt);
-                  sm.gkey[slot] = ck;
-                  sm.gid[slot] = id;
-                } else {
-                  const int c = bc + __popc(mc & lt);
-                  if (c < kCandCap) {
-                    ckey[c] = ck;
-                    cid[c] = id;
-                  }
+              if (u >= NK || kk[i] < lo_key) continue;
+              const int g = f * SS + flat_in_face<S>(tid, u);
+              const uint64_t ck = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
+              const int id = (f * NK + u) * kThreads + tid;
+              if (kk[i] >= hi_key) {
+                const int slot = atomicAdd(&sm.scal[kScNAbove], 1);
+                sm.gkey[slot] = ck;
+                sm.gid[slot] = id;
+              } else {
+                const int c = atomicAdd(&sm.scal[kScNCand], 1);
+                if (c < kCandCap) {
+                  ckey[c] = ck;
+                  cid[c] = id;
                 }
               }
             }
