@@ -65,12 +65,20 @@ def test_haar_topk_batched_and_single_map_forms_agree(cuda, S, K):
     faces[7] = 1.0                                                      # constant map
     faces[9, 1, 0, 0, 0] = np.nan
     faces[11, 4, S - 1, S - 1, 2] = np.inf
+    # the selection's shortcuts: winners packed into a few texel blocks (the per-block maxima
+    # bound the threshold loosely), a dynamic range wider than the first pass's window (fewer
+    # than K keys in it: the full passes run), all zeros, negative texels
+    h = max(1, S // 4)
+    faces[13, 2, :h, :h, :] *= 1e4
+    faces[15, 0, 0, 0, :] = 1e30
+    faces[17] = 0.0
+    faces[19] = -faces[19]
     tf = torch.from_numpy(faces).to(cuda)
     idx, st = _engine().haar_topk(tf, K)
     ridx, rst = O.haar_topk(faces, K)
     assert np.array_equal(idx.cpu().numpy(), ridx)
     assert bits_equal(st.cpu().numpy(), rst)
-    for e in (0, 3, 7, 9, 11, E - 1):
+    for e in (0, 3, 7, 9, 11, 13, 15, 17, E - 1):
         i1, s1 = _engine().haar_topk(tf[e:e + 1].contiguous(), K)
         assert np.array_equal(i1.cpu().numpy()[0], ridx[e]), e
         assert bits_equal(s1.cpu().numpy()[0], rst[e]), e
