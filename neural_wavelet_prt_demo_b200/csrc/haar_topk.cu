@@ -591,6 +591,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr int NW = (6 * SS + 31) / 32;
   static_assert(T <= kThreads, "one 4x4 block per thread");
   static_assert(kThreads == 256, "one thread per bin of the winners' counting pass");
+  static_assert(3 * FaceGeom<S>::G * FaceGeom<S>::G * sizeof(float) <= kWarps * 256 * sizeof(uint32_t),
+                "the second `upper` buffer fits the histogram region");
   static_assert(512 * sizeof(uint32_t) + kMaxK * sizeof(uint16_t) <= kWarps * 256 * sizeof(uint32_t),
                 "the winners' bins and order fit the histogram region");
   extern __shared__ __align__(16) char smem_raw[];
@@ -614,15 +616,19 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (nxt < (long long)n_env * 6 && (reinterpret_cast<uintptr_t>(pf) & 15) == 0)
           asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(pf), "r"((uint32_t)(SS * 12)) : "memory");
       }
+      // `upper` alternates between two buffers (the second is the histogram region, idle until
+      // the select): a face overwrites only the buffer of the face before last, whose readers
+      // all passed the last face's barriers, so faces need no barrier of their own
+      float* upper = (f & 1) ? reinterpret_cast<float*>(sm.whist) : sm.upper;
       float co[NR > 0 ? NR : 1][3];
-      haar_face_in_registers<S>(src, tid, co, sm.upper, sm.llg);
+      haar_face_in_registers<S>(src, tid, co, upper, sm.llg);
       uint32_t k[NKQ * 4];
 #pragma unroll
       for (int u = 0; u < NKQ * 4; ++u) k[u] = 0u;
       if (owner) {
 #pragma unroll
         for (int u = 0; u < NR; ++u) k[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
-        const float ur = sm.upper[tid * 3], ug = sm.upper[tid * 3 + 1], ub = sm.upper[tid * 3 + 2];
+        const float ur = upper[tid * 3], ug = upper[tid * 3 + 1], ub = upper[tid * 3 + 2];
         k[NR] = wavelet_key_bits(ur, ug, ub);
 #pragma unroll
         for (int u = 0; u <= NR; ++u) kmax = max(kmax, k[u]);
@@ -633,8 +639,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
       for (int q = 0; q < NKQ; ++q)
         sm.keys[((size_t)f * NKQ + q) * kThreads + tid] = make_uint4(k[4 * q], k[4 * q + 1], k[4 * q + 2], k[4 * q + 3]);
-      __syncthreads();  // the next face reuses `upper`
     }
+    __syncthreads();  // the last face's `upper` (the histogram region) is read; the select reuses it
     // ---- radix select of the K-th largest key.  The keys' top bits are mostly exponent, so a
     // plain first pass piles 24K keys into a few bins (serialised shared atomics).  Instead the
     // first pass histograms only keys within 16 binades of the largest key, at 1/16 binade
