@@ -240,8 +240,11 @@ __device__ __forceinline__ void block_coef(const float* __restrict__ src, int ti
 // levels 1-2 on each thread's B x B block in registers (co: its NR detail coefficients),
 // the next levels by warp shuffles, the last ones in warp 0.  The G x G upper block of the
 // result (levels >= 3 and the DC term) lands in `upper` [G*G][3]; `llg` is [16][3] staging.
-// Ends with a block barrier, after which `upper` is complete.
-template <int S>
+// Ends with a block barrier, after which `upper` is complete.  PARTIAL_TAIL (for S >= 32, where
+// the last levels run in warp 0 after a block barrier): only the warps whose own upper-block
+// entries those levels write wait for them, on a named barrier; every other entry was written
+// before the block barrier.  The caller then alternates `upper` and `llg` between two buffers.
+template <int S, bool PARTIAL_TAIL = false>
 __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__ src, int tid,
                                                        float (&co)[FaceGeom<S>::NR > 0 ? FaceGeom<S>::NR : 1][3],
                                                        float* upper, float* llg) {
@@ -357,7 +360,14 @@ __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__
       for (int c = 0; c < 3; ++c) upper[c] = ll[c];
     }
   }
-  __syncthreads();
+  if constexpr (PARTIAL_TAIL && G >= 8) {
+    // warp 0 finished an n x n LL grid, n = G / 4: it wrote entries (i, j), i, j < n, read by
+    // threads i * G + j, i.e. the first NT warps
+    constexpr int n = G / 4, NT = ((n - 1) * G + n - 1) / 32 + 1;
+    if (warp < NT) asm volatile("bar.sync 1, %0;" ::"n"(NT * 32) : "memory");
+  } else {
+    __syncthreads();
+  }
 }
 
 template <int S>
@@ -540,7 +550,7 @@ struct BatchSmem {
   uint64_t* gkey;   // [K]
   int* gid;         // [K] winner: (face * NK + u) * kThreads + thread
   float* upper;     // [(S/4)^2][3]
-  float* llg;       // [16][3]
+  float* llg;       // [2][16][3], alternating by face
   int* warp_tot;
   int* scal;
 };
@@ -558,7 +568,7 @@ __host__ __device__ inline size_t batch_smem_layout(int S, int K, char* base, Ba
   const size_t oG = take(sizeof(uint64_t) * K);
   const size_t oI = take(sizeof(int) * K);
   const size_t oU = take(sizeof(float) * 3 * G * G);
-  const size_t oL = take(sizeof(float) * 3 * 16);
+  const size_t oL = take(sizeof(float) * 3 * 16 * 2);
   const size_t oW = take(sizeof(int) * kWarps);
   const size_t oS = take(sizeof(int) * 32);
   if (L) {
@@ -621,7 +631,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       // all passed the last face's barriers, so faces need no barrier of their own
       float* upper = (f & 1) ? reinterpret_cast<float*>(sm.whist) : sm.upper;
       float co[NR > 0 ? NR : 1][3];
-      haar_face_in_registers<S>(src, tid, co, upper, sm.llg);
+      haar_face_in_registers<S, true>(src, tid, co, upper, sm.llg + (f & 1) * 48);
       uint32_t k[NKQ * 4];
 #pragma unroll
       for (int u = 0; u < NKQ * 4; ++u) k[u] = 0u;
