@@ -175,6 +175,10 @@ struct TcPlan {
   uint32_t blob_bytes = 0;
   float cp_scale = 1.f;     // FP8: scale of the first layer's operand hash(p) * E_k
   float vlast[3][64] = {};  // V_last, FP32 [c][j] (filled when the weights are given)
+  // BF16 plans: V_last as FP16 B tile of the output layer on the tensor core (N=16: channel c
+  // in row c, K = the last hidden width padded to 16), at out_b_off with 8-row stride out_sbo
+  uint32_t out_b_off = 0, out_sbo = 0;
+  int out_k = 0;
 };
 enum TcMode { kTcBf16 = 0, kTcCalibrate = 1, kTcFp8 = 2 };
 bool relight_tc_supported(const NetDims& d, std::string* why);

@@ -73,6 +73,7 @@ struct TcParams {
   const float* hash;
   uint32_t wblob_bytes;
   uint32_t w_boxes, w_box_rows;
+  uint32_t out_b_off, out_sbo;  // BF16: the output layer's FP16 B tile (V_last) in the blob
   TcLayer layers[kMaxTcLayers];
   int n_layers;
   int enc_dims;  // D, multiple of 16, <= 32
@@ -158,6 +159,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
+// kind::f16 instruction descriptor: D=F32, A=B=F16 (format code 0), both K-major, M=128.
+__host__ __device__ constexpr uint32_t idesc_f16(int n) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
 // kind::f8f6f4 instruction descriptor: D=F32, A=B=E4M3 (format code 0), both K-major, M=128.
 __host__ __device__ constexpr uint32_t idesc_e4m3(int n) {
   return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
@@ -226,6 +231,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 }
 
 
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
@@ -248,6 +259,13 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 __device__ __forceinline__ uint32_t pack_bf16_relu(float lo, float hi) {
   uint32_t d;
   asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+// ReLU(lo), ReLU(hi) -> an FP16 pair (round to nearest even, saturated to the largest finite
+// FP16), lo in the low half.
+__device__ __forceinline__ uint32_t pack_f16_relu(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.satfinite.relu.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
 // Four FP32 values -> four E4M3 bytes (round to nearest even, saturated to +-448), x0 in
@@ -321,6 +339,12 @@ __device__ __forceinline__ void pack32(const uint32_t (&v)[32], uint32_t* out) {
     const float lo = __uint_as_float(v[2 * j]), hi = __uint_as_float(v[2 * j + 1]);
     out[j] = RELU ? pack_bf16_relu(lo, hi) : pack_bf16(lo, hi);
   }
+}
+
+// 32 FP32 TMEM values -> 16 ReLU'd FP16 pairs.
+__device__ __forceinline__ void pack32_f16_relu(const uint32_t (&v)[32], uint32_t* out) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) out[j] = pack_f16_relu(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
 }
 
 // Two FP32 values in one 64-bit register, for the packed f32x2 arithmetic of sm_100.
@@ -538,10 +562,23 @@ __device__ __forceinline__ void issue_layer(const TcLayer& L, bool with_aux, uin
   mma_commit(bar);
 }
 
+// The output layer T = V_last ReLU(h) on the tensor core: A = the last hidden layer's ReLU'd
+// activations as FP16 pairs in TMEM, B = V_last in FP16 (N = 16, channel c in row c), K = 64.
+__device__ __forceinline__ void issue_out(uint32_t wbase, uint32_t b_off, uint32_t sbo, uint32_t a_tmem,
+                                          uint32_t d_tmem, uint64_t* bar) {
+  tc_fence_after();
+  issue_steps<kTcBf16, 4>(d_tmem, a_tmem, smem_desc(wbase + b_off, 128u, sbo), idesc_f16(16));
+  mma_commit(bar);
+}
+
 template <int DMAX, int MODE, int SHAPE>
 __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_constant__ TcParams p) {
   using Sh = ShapeOf<SHAPE>;
+  // BF16 with a fixed layer sequence: the 64 -> 3 output layer is one more tensor-core step
+  // (FP16 operands, FP32 accumulation) instead of an FP32 dot on the CUDA cores
+  constexpr bool OUT_TC = MODE == kTcBf16 && SHAPE != kShapePlan;
   const int n_layers = SHAPE ? Sh::nl : p.n_layers;
+  const int n_steps = n_layers + (OUT_TC ? 1 : 0);  // tensor-core steps per wavelet
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;                                                  // weight blob
   uint8_t* aux = smem + weight_region_bytes(p.w_boxes, p.w_box_rows);  // [kNWG][kAuxBytes]
@@ -627,11 +664,34 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     if (ok && q == 0 && elect_one())
       issue_layer<MODE>(p.layers[0], SHAPE ? Sh::aux == 0 : p.layers[0].aux != 0, wbase, a_tmem, aux_base, d_tmem,
                         acc_bar);
+    // T_k -> clamped Kahan sums, then the next wavelet's first-layer operand
+    auto finish_wavelet = [&](int k, float t0, float t1, float t2) {
+      const float* Lk = J.strength + (size_t)k * 3;
+      float u0 = __fmul_rn(__ldg(Lk + 0), t0);
+      float u1 = __fmul_rn(__ldg(Lk + 1), t1);
+      float u2 = __fmul_rn(__ldg(Lk + 2), t2);
+      if (p.clamp) { u0 = fmaxf(u0, 0.f); u1 = fmaxf(u1, 0.f); u2 = fmaxf(u2, 0.f); }
+      if (p.kahan) {
+        float y, z;
+        y = __fsub_rn(u0, c0); z = __fadd_rn(s0, y); c0 = __fsub_rn(__fsub_rn(z, s0), y); s0 = z;
+        y = __fsub_rn(u1, c1); z = __fadd_rn(s1, y); c1 = __fsub_rn(__fsub_rn(z, s1), y); s1 = z;
+        y = __fsub_rn(u2, c2); z = __fadd_rn(s2, y); c2 = __fsub_rn(__fsub_rn(z, s2), y); s2 = z;
+      } else {
+        s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
+      }
+      if (k + 1 < K) {
+        store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims,
+                             J.emb_h + (size_t)(k + 1) * (p.enc_dims / 2), a_taddr, p.cp_scale, p.amax);
+        tmem_wait_st();
+      }
+    };
     for (int k = 0; k < K && ok; ++k) {
-#pragma unroll(SHAPE ? Sh::nl : 1)
-      for (int l = 0; l < n_layers; ++l) {
-        const TcLayer& L = p.layers[l];
-        const bool fin = SHAPE ? l == Sh::nl - 1 : L.fin != 0;
+#pragma unroll(SHAPE ? Sh::nl + (OUT_TC ? 1 : 0) : 1)
+      for (int l = 0; l < n_steps; ++l) {
+        const TcLayer& L = p.layers[l < n_layers ? l : 0];
+        const bool is_out = OUT_TC && l == n_layers;       // the output layer's accumulator
+        const bool pre_out = OUT_TC && l == n_layers - 1;  // the last hidden layer, packed as FP16
+        const bool fin = !OUT_TC && (SHAPE ? l == Sh::nl - 1 : L.fin != 0);
         const bool relu = SHAPE ? true : L.relu != 0;
         const bool wide_out = SHAPE ? true : L.n > 32;
         const bool waited = __all_sync(0xffffffffu, wait_bounded(acc_bar, ph, p.err));
@@ -639,7 +699,23 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         if (waited) {
           tc_fence_after();
           uint32_t v[32];
-          if (!fin && MODE == kTcFp8) {
+          if (is_out) {
+            uint32_t t[4];
+            tmem_ld4(d_taddr, t);
+            tmem_wait_ld();
+            finish_wavelet(k, __uint_as_float(t[0]), __uint_as_float(t[1]), __uint_as_float(t[2]));
+          } else if (pre_out) {
+            uint32_t a[16];
+            tmem_ld32(d_taddr, v);
+            tmem_wait_ld();
+            pack32_f16_relu(v, a);
+            tmem_st16(a_taddr, a);
+            tmem_ld32(d_taddr + 32u, v);
+            tmem_wait_ld();
+            pack32_f16_relu(v, a);
+            tmem_st16(a_taddr + 16u, a);
+            tmem_wait_st();
+          } else if (!fin && MODE == kTcFp8) {
             uint32_t a[8];
             tmem_ld32(d_taddr, v);
             tmem_wait_ld();
@@ -686,35 +762,22 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             if constexpr (MODE == kTcCalibrate) record_amax(p.amax + n_layers, max(m, amax32(v, true)));
             final_dot32x2(v, p.vlast, 32, q0, q1, q2);
             t0 = sum2(q0); t1 = sum2(q1); t2 = sum2(q2);
-            const float* Lk = J.strength + (size_t)k * 3;
-            float u0 = __fmul_rn(__ldg(Lk + 0), t0);
-            float u1 = __fmul_rn(__ldg(Lk + 1), t1);
-            float u2 = __fmul_rn(__ldg(Lk + 2), t2);
-            if (p.clamp) { u0 = fmaxf(u0, 0.f); u1 = fmaxf(u1, 0.f); u2 = fmaxf(u2, 0.f); }
-            if (p.kahan) {
-              float y, z;
-              y = __fsub_rn(u0, c0); z = __fadd_rn(s0, y); c0 = __fsub_rn(__fsub_rn(z, s0), y); s0 = z;
-              y = __fsub_rn(u1, c1); z = __fadd_rn(s1, y); c1 = __fsub_rn(__fsub_rn(z, s1), y); s1 = z;
-              y = __fsub_rn(u2, c2); z = __fadd_rn(s2, y); c2 = __fsub_rn(__fsub_rn(z, s2), y); s2 = z;
-            } else {
-              s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
-            }
-            if (k + 1 < K) {
-              store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims,
-                                   J.emb_h + (size_t)(k + 1) * (p.enc_dims / 2), a_taddr, p.cp_scale, p.amax);
-              tmem_wait_st();
-            }
+            finish_wavelet(k, t0, t1, t2);
           }
         }
         ok = ok && waited;
-        if (l + 1 == n_layers && k + 1 == K) break;  // the tile's last layer: no hand-off
-        const int nl = (l + 1 == n_layers) ? 0 : l + 1;
+        if (l + 1 == n_steps && k + 1 == K) break;  // the tile's last step: no hand-off
+        const int nl = (l + 1 == n_steps) ? 0 : l + 1;
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
         if (!ok) break;
-        if (q == 0 && elect_one())
-          issue_layer<MODE>(p.layers[nl], SHAPE ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
-                            d_tmem, acc_bar);
+        if (q == 0 && elect_one()) {
+          if (OUT_TC && nl == n_layers)
+            issue_out(wbase, p.out_b_off, p.out_sbo, a_tmem, d_tmem, acc_bar);
+          else
+            issue_layer<MODE>(p.layers[nl], SHAPE ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
+                              d_tmem, acc_bar);
+        }
       }
     }
     if (valid && ok) {
@@ -772,6 +835,25 @@ uint8_t to_e4m3(float f) {
   return sign | (uint8_t)(((E + 7) << 3) | (int)q);
 }
 
+// FP32 -> FP16 (1 sign, 5 exponent bits with bias 15, 10 mantissa bits), round to nearest
+// even, overflow to infinity.
+uint16_t to_f16(float f) {
+  if (std::isnan(f)) return 0x7e00;
+  const uint16_t sign = std::signbit(f) ? 0x8000 : 0x0000;
+  const double a = std::fabs((double)f);
+  if (a >= 65520.0) return sign | 0x7c00;  // 65520 = halfway between 65504 and the next step
+  if (a < std::ldexp(1.0, -14)) return sign | (uint16_t)std::nearbyint(a * 16777216.0);  // multiples of 2^-24
+  int e;
+  const double m = std::frexp(a, &e);  // a = m * 2^e, m in [0.5, 1)
+  double q = std::nearbyint((m * 2.0 - 1.0) * 1024.0);
+  int E = e - 1;
+  if (q >= 1024.0) {
+    q = 0.0;
+    ++E;
+  }
+  return sign | (uint16_t)(((E + 15) << 10) | (int)q);
+}
+
 int pad16(int x) { return (x + 15) & ~15; }
 int pad32(int x) { return (x + 31) & ~31; }
 
@@ -780,7 +862,7 @@ int pad32(int x) { return (x + 31) & ~31; }
 // Core matrices are 8 rows x 16 bytes; K-adjacent ones are 128 bytes apart, 8-row groups
 // kp * eb * 8 bytes apart.
 void put_b(std::vector<uint8_t>* blob, size_t off, const float* src, int n, int k_total, int col0, int kc,
-           int np, int kp, int eb, float scale) {
+           int np, int kp, int eb, float scale, bool f16 = false) {
   const size_t need = off + (size_t)np * kp * eb;
   if (blob->size() < need) blob->resize(need, 0);
   const size_t sbo = (size_t)kp * eb * 8;
@@ -790,7 +872,7 @@ void put_b(std::vector<uint8_t>* blob, size_t off, const float* src, int n, int 
       const size_t cb = (size_t)c * eb;  // byte column within the row
       const size_t byte = off + (size_t)(r >> 3) * sbo + (cb >> 4) * 128 + (size_t)(r & 7) * 16 + (cb & 15);
       if (eb == 2) {
-        const uint16_t h = to_bf16(v);
+        const uint16_t h = f16 ? to_f16(v) : to_bf16(v);
         std::memcpy(blob->data() + byte, &h, 2);
       } else {
         (*blob)[byte] = to_e4m3(v);
@@ -895,6 +977,17 @@ TcPlan make_plan(const NetDims& d, const float* op, const float* cn, int eb, con
     const float inv = eb == 2 ? 1.f : 1.f / dscale[P.n_layers - 1];
     for (int c = 0; c < 3; ++c)
       for (int j = 0; j < 64; ++j) P.vlast[c][j] = j < n_in ? w[(size_t)c * n_in + j] * inv : 0.f;
+  }
+  // BF16: V_last as the FP16 B tile of the output layer on the tensor core (N = 16, channel c in
+  // row c; FP16 keeps 11 significant bits of ReLU(h) and V_last, where BF16 keeps 8)
+  if (eb == 2) {
+    const int n_in = d.cn_in[d.cn_nl - 1], kp = pad16(n_in);
+    P.out_b_off = (uint32_t)off;
+    P.out_sbo = (uint32_t)(kp * 2 * 8);
+    P.out_k = kp;
+    if (fill) put_b(blob, off, vlast_src(d, cn), 3, n_in, 0, n_in, 16, kp, 2, 1.f, true);
+    off += (size_t)16 * kp * 2;
+    off = (off + 127) & ~size_t(127);
   }
   if (blob) blob->resize(off, 0);
   P.blob_bytes = (uint32_t)off;
@@ -1087,6 +1180,8 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.hl = hl;
   p.hash = hash;
   p.wblob_bytes = P.blob_bytes;
+  p.out_b_off = P.out_b_off;
+  p.out_sbo = P.out_sbo;
   encode_weight_map(&p.wmap, blob_dev, P.blob_bytes, &p.w_boxes, &p.w_box_rows);
   std::memcpy(p.vlast, P.vlast, sizeof(p.vlast));
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
@@ -1120,6 +1215,8 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
     kern<<<grid, kThreads, smem, st>>>(p);
   };
   const int shape = shape_of(P, d);
+  if (mode == kTcBf16 && shape != kShapePlan && (P.out_k != 64 || P.out_sbo == 0))
+    fail(NWPRT_INVALID_ARG, "tensor-core relight: the BF16 plan lacks its 64-wide FP16 output tile");
   auto pick = [&](auto mode_tag) {
     constexpr int M = decltype(mode_tag)::value;
     if (shape == kShapeSix) go(relight_tc_kernel<32, M, kShapeSix>);
