@@ -5,8 +5,12 @@
 // -> cmp_net MLP -> T_k, and sum_k max(L_k * T_k, 0).  Every hidden dense layer of a
 // 128-pixel x 1-wavelet row block is one tcgen05.mma chain (M=128, N<=64, K=16 steps);
 // out_prd's linear output layer is folded into cmp_net's first layer on the host (one
-// round trip less per wavelet); the final 3-output layer runs in FP32 on the CUDA cores
-// inside the epilogue of the layer before it, straight from the FP32 accumulator.
+// round trip less per wavelet).  The final 3-output layer is one more tensor-core step in the
+// BF16 kernels with a fixed layer sequence: the last hidden layer's ReLU'd activations go back
+// to TMEM as FP16 pairs and meet V_last in FP16 (N = 16, FP32 accumulation; FP16 keeps 11
+// significant bits where BF16 keeps 8, so the output layer loses nothing measurable).  The
+// FP8, calibration and generic forms run it in FP32 on the CUDA cores inside the epilogue of
+// the layer before it, straight from the FP32 accumulator.
 //
 // Design, from measurements on B200: an M=128 N=64 tcgen05.mma issued back to back from an
 // elected lane of a converged warp takes ~36 cycles (~90% of the tensor peak), and five
@@ -28,8 +32,9 @@
 // layer: wait on the tile's commit barrier -> tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 ->
 // tcgen05.st into the A columns -> warpgroup barrier (bar.red.and carrying the "no
 // timeout" vote) -> an elected lane of warp 0 issues the next layer's MMAs and commits
-// them.  The final layer's epilogue forms T_k, does the clamped Kahan sum and writes the
-// next wavelet's first-layer operand hash(p) * E_k+1.  The two standard networks run
+// them.  The output layer's epilogue (or, in the FP32-dot forms, the last
+// hidden layer's) forms T_k, does the clamped Kahan sum and writes the next wavelet's
+// first-layer operand hash(p) * E_k+1.  The two standard networks run
 // kernels specialised on their layer sequence (ShapeOf), every other supported network a
 // generic form that reads the sequence from the plan.  Every wait is bounded by
 // %globaltimer (2 s); on expiry the kernel records kDevWaitTimeout and the warpgroup
