@@ -684,7 +684,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
       } else {
         s0 = __fadd_rn(s0, u0); s1 = __fadd_rn(s1, u1); s2 = __fadd_rn(s2, u2);
       }
-      if (k + 1 < K) {
+      if (!OUT_TC && k + 1 < K) {  // OUT_TC: written while the output layer's MMA runs
         store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims,
                              J.emb_h + (size_t)(k + 1) * (p.enc_dims / 2), a_taddr, p.cp_scale, p.amax);
         tmem_wait_st();
@@ -710,15 +710,18 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             tmem_wait_ld();
             finish_wavelet(k, __uint_as_float(t[0]), __uint_as_float(t[1]), __uint_as_float(t[2]));
           } else if (pre_out) {
+            // the output layer's operand goes to accumulator columns [64, 96) (the second half
+            // is read before its columns are overwritten), leaving the A columns free for the
+            // next wavelet's first-layer operand while the output MMA runs
             uint32_t a[16];
-            tmem_ld32(d_taddr, v);
-            tmem_wait_ld();
-            pack32_f16_relu(v, a);
-            tmem_st16(a_taddr, a);
             tmem_ld32(d_taddr + 32u, v);
             tmem_wait_ld();
             pack32_f16_relu(v, a);
-            tmem_st16(a_taddr + 16u, a);
+            tmem_st16(d_taddr + 48u, a);
+            tmem_ld32(d_taddr, v);
+            tmem_wait_ld();
+            pack32_f16_relu(v, a);
+            tmem_st16(d_taddr + 32u, a);
             tmem_wait_st();
           } else if (!fin && MODE == kTcFp8) {
             uint32_t a[8];
@@ -778,10 +781,17 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         if (!ok) break;
         if (q == 0 && elect_one()) {
           if (OUT_TC && nl == n_layers)
-            issue_out(wbase, p.out_b_off, p.out_sbo, a_tmem, d_tmem, acc_bar);
+            issue_out(wbase, p.out_b_off, p.out_sbo, d_tmem + 32u, d_tmem, acc_bar);
           else
             issue_layer<MODE>(p.layers[nl], SHAPE ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
                               d_tmem, acc_bar);
+        }
+        if (OUT_TC && nl == n_layers && k + 1 < K) {
+          // the next wavelet's first-layer operand into the A columns, which the output MMA
+          // (operand in [64, 96), accumulator in [32, 48)) does not touch
+          store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims,
+                               J.emb_h + (size_t)(k + 1) * (p.enc_dims / 2), a_taddr, p.cp_scale, p.amax);
+          tmem_wait_st();
         }
       }
     }
