@@ -690,6 +690,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         tmem_wait_st();
       }
     };
+    float tk0 = 0.f, tk1 = 0.f, tk2 = 0.f;  // OUT_TC: T_k, summed after the next hand-off
     for (int k = 0; k < K && ok; ++k) {
 #pragma unroll(SHAPE ? Sh::nl + (OUT_TC ? 1 : 0) : 1)
       for (int l = 0; l < n_steps; ++l) {
@@ -708,7 +709,9 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             uint32_t t[4];
             tmem_ld4(d_taddr, t);
             tmem_wait_ld();
-            finish_wavelet(k, __uint_as_float(t[0]), __uint_as_float(t[1]), __uint_as_float(t[2]));
+            tk0 = __uint_as_float(t[0]);
+            tk1 = __uint_as_float(t[1]);
+            tk2 = __uint_as_float(t[2]);
           } else if (pre_out) {
             // the output layer's operand goes to accumulator columns [64, 96) (the second half
             // is read before its columns are overwritten), leaving the A columns free for the
@@ -774,7 +777,10 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
           }
         }
         ok = ok && waited;
-        if (l + 1 == n_steps && k + 1 == K) break;  // the tile's last step: no hand-off
+        if (l + 1 == n_steps && k + 1 == K) {  // the tile's last step: no hand-off
+          if (is_out && waited) finish_wavelet(k, tk0, tk1, tk2);
+          break;
+        }
         const int nl = (l + 1 == n_steps) ? 0 : l + 1;
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
@@ -786,6 +792,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
             issue_layer<MODE>(p.layers[nl], SHAPE ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
                               d_tmem, acc_bar);
         }
+        if (is_out) finish_wavelet(k, tk0, tk1, tk2);  // under the next wavelet's first MMA
         if (OUT_TC && nl == n_layers && k + 1 < K) {
           // the next wavelet's first-layer operand into the A columns, which the output MMA
           // (operand in [64, 96), accumulator in [32, 48)) does not touch
