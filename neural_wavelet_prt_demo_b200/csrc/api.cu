@@ -3,6 +3,7 @@
 // Mirrors the reference's engine entry points (Renderer/RenderEngine.h:78-83,
 // Renderer/tinycudann/tcnn.cu:49-162) behind status codes: nothing throws across the
 // boundary, every failure leaves a message in nwprt_last_error().
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -101,6 +102,11 @@ struct nwprt_ctx {
   std::vector<EnvEntry> envs;
   Frame frames[NWPRT_MAX_FRAMES];
   uint32_t* d_err = nullptr;
+  // Tile counters of the tensor-core relight (its warpgroups take tiles from one counter per
+  // launch): a ring, so that launches in flight on different streams use different counters.
+  static constexpr int kTileCounters = 64;
+  int* d_tile_ctr = nullptr;
+  int tile_ctr_next = 0;
   float* d_stage = nullptr;
   size_t stage_cap = 0;
 
@@ -113,6 +119,7 @@ struct nwprt_ctx {
     dev_free(d_tc_w);
     dev_free(d_tc_w8);
     dev_free(d_err);
+    dev_free(d_tile_ctr);
     dev_free(d_stage);
     for (auto& e : envs) free_env_buffers(e);
     for (auto& f : frames) dev_free(f.packed);
@@ -186,31 +193,35 @@ void ensure_emb(nwprt_ctx* ctx, EnvEntry& e, cudaStream_t st) {
   e.emb_ready = true;
 }
 
-// Registers an env slot for K wavelets.  Released slots are reused in stream order: a slot
-// whose buffers hold >= K wavelets is taken without any allocation, so a serving loop that
-// registers and releases env maps per request does not allocate or synchronise.
+// Registers an env slot for K wavelets.  Released slots are reused in stream order without
+// any allocation or synchronisation: a slot holds kEnvSlotWavelets wavelets (or K, if larger;
+// ~200 KB at 32 hash features), so any released slot fits any K the Haar path produces.  A K
+// that no released slot fits gets a new slot; slots are freed with the context.  (Replacing a
+// smaller slot would need a device-wide synchronisation before its buffers could be freed,
+// which drains a serving loop's queue of launches.)
+constexpr int kEnvSlotWavelets = 1024;
+
 int new_env(nwprt_ctx* ctx, int K, int D) {
-  int id = -1, spare = -1;
+  int id = -1;
   for (size_t i = 0; i < ctx->envs.size(); ++i) {
     const EnvEntry& e = ctx->envs[i];
-    if (e.live) continue;
-    if (e.cap >= K && (id < 0 || e.cap < ctx->envs[id].cap)) id = (int)i;
-    if (spare < 0) spare = (int)i;
+    if (e.live || e.cap < K) continue;
+    if (id < 0 || e.cap < ctx->envs[id].cap) id = (int)i;
   }
   if (id < 0) {
-    if (spare >= 0) {
-      NWPRT_CUDA(cudaDeviceSynchronize());  // buffers too small: replace them
-      free_env_buffers(ctx->envs[spare]);
-      id = spare;
-    } else {
-      ctx->envs.emplace_back();
-      id = (int)ctx->envs.size() - 1;
+    const int cap = std::max(K, kEnvSlotWavelets);
+    EnvEntry e;
+    try {
+      e.idx = dev_alloc<int32_t>(cap);
+      e.strength = dev_alloc<float>((size_t)cap * 3);
+      e.emb_k = dev_alloc<float>((size_t)cap * D + (size_t)cap * (D / 2));
+    } catch (...) {
+      free_env_buffers(e);
+      throw;
     }
-    EnvEntry& e = ctx->envs[id];
-    e.idx = dev_alloc<int32_t>(K);
-    e.strength = dev_alloc<float>((size_t)K * 3);
-    e.emb_k = dev_alloc<float>((size_t)K * D + (size_t)K * (D / 2));
-    e.cap = K;
+    e.cap = cap;
+    ctx->envs.push_back(e);
+    id = (int)ctx->envs.size() - 1;
   }
   EnvEntry& e = ctx->envs[id];
   e.K = K;
@@ -282,6 +293,7 @@ nwprt_status nwprt_create(const char* config_json, int device, nwprt_ctx** out) 
     c->tc_supported = relight_tc_supported(d, &c->tc_why);
     c->d_err = dev_alloc<uint32_t>(1);
     NWPRT_CUDA(cudaMemset(c->d_err, 0, sizeof(uint32_t)));
+    c->d_tile_ctr = dev_alloc<int>(nwprt_ctx::kTileCounters);
     *out = c.release();
   });
 }
@@ -564,12 +576,14 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
                          0, r.px_begin, emb_pairs(e, ctx->dims.enc_dims())});
   }
   if (jobs.empty()) return;
+  int* ctr = ctx->d_tile_ctr + ctx->tile_ctr_next;
+  ctx->tile_ctr_next = (ctx->tile_ctr_next + 1) % nwprt_ctx::kTileCounters;
   if (mode == kTcFp8)
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w8, &ctx->fp8_plan, mode, jobs.data(),
-                      (int)jobs.size(), o.kahan, o.clamp_terms, nullptr, ctx->d_err, st);
+                      (int)jobs.size(), o.kahan, o.clamp_terms, nullptr, ctx->d_err, ctr, st);
   else
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w, &ctx->bf16_plan, mode, jobs.data(),
-                      (int)jobs.size(), o.kahan, o.clamp_terms, amax, ctx->d_err, st);
+                      (int)jobs.size(), o.kahan, o.clamp_terms, amax, ctx->d_err, ctr, st);
 }
 
 static void relight_ranges(nwprt_ctx* ctx, const std::vector<RangeReq>& reqs, const nwprt_relight_opts& o,

@@ -213,10 +213,12 @@ struct TcJob {
 };
 // mode kTcBf16 / kTcCalibrate use the BF16 blob and its plan (from pack_tc_weights);
 // kTcCalibrate also records per-layer activation maxima into amax (uint bits of floats);
-// kTcFp8 uses the FP8 blob and its plan.
+// kTcFp8 uses the FP8 blob and its plan.  tile_ctr: one device int, reset on `st` before
+// each kernel launch; the kernel's warpgroups take 128-pixel tiles from it, so no other
+// launch may use it while this one runs.
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
                        const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, int kahan, int clamp,
-                       uint32_t* amax, uint32_t* err, cudaStream_t st);
+                       uint32_t* amax, uint32_t* err, int* tile_ctr, cudaStream_t st);
 
 }  // namespace nwprt
 

@@ -89,6 +89,7 @@ struct TcParams {
   float cp_scale;   // FP8: scale of the first layer's operand
   uint32_t* amax;   // calibration: per-layer activation maxima (float bits)
   uint32_t* err;
+  int* tile_ctr;    // the next 128-pixel tile to take (zeroed before the launch)
   // V_last, the FP32 3 x 64 output layer.  From the parameter space every output-dot FMA
   // takes its weight pair as an operand, without a shared-memory load.
   float vlast[3][64];
@@ -502,6 +503,7 @@ struct __align__(8) TcBarriers {
   uint64_t done[kNWG];      // final commit before TMEM is released
   uint64_t wload;           // the weight blob's TMA load
   uint32_t tmem_base;
+  int tile_slot[kNWG];      // the tile each warpgroup took from the launch's counter
 };
 
 // Shared-memory bytes of the weight region: whole TMA boxes, rounded to 1 KB.
@@ -621,7 +623,6 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   bool ok = wait_bounded(&bars->wload, 0, p.err);
   const uint32_t tmem = bars->tmem_base;
   const uint32_t wbase = smem_u32(wsm);
-  const long long stride = (long long)gridDim.x * kNWG;
   const uint32_t col0 = tmem + (uint32_t)(g * kTileCols);
   const uint32_t a_tmem = col0 + kAcol;                                 // MMA operand address (lane 0)
   const uint32_t d_tmem = col0 + kDcol;
@@ -632,8 +633,13 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   uint64_t* acc_bar = &bars->acc_full[g];
 
   uint32_t ph = 0;
+  // Tiles come from the launch's counter, one atomic per tile and warpgroup, so that tiles of
+  // different cost (jobs of different K or pixel count; the host puts the longest tiles first)
+  // balance across the SMs.  The slot is read after a warpgroup barrier and rewritten only after
+  // the next one (every tile has at least one).
+  if (q == 0 && lane == 0) bars->tile_slot[g] = atomicAdd(p.tile_ctr, 1);
   ok = wg_barrier_and(g, ok);
-  for (long long t = (long long)blockIdx.x * kNWG + g; t < p.total_tiles && ok; t += stride) {
+  for (long long t = bars->tile_slot[g]; t < p.total_tiles && ok; t = bars->tile_slot[g]) {
     // ---- tile set-up: hash encoding, aux operand, first-layer operand of wavelet 0
     const int jid = find_job(p.jobs, p.n_jobs, t);
     const TcJob& J = p.jobs[jid];
@@ -809,7 +815,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
       reinterpret_cast<float4*>(J.with_direct)[px] =
           make_float4(__fadd_rn(ind.x, dl.x), __fadd_rn(ind.y, dl.y), __fadd_rn(ind.z, dl.z), 1.f);
     }
-    // every thread of the warpgroup agrees on the outcome before the next tile
+    // every thread of the warpgroup agrees on the outcome (and sees the next tile) before it
+    if (q == 0 && lane == 0) bars->tile_slot[g] = atomicAdd(p.tile_ctr, 1);
     ok = wg_barrier_and(g, ok);
   }
   // every MMA this warpgroup issued has completed before TMEM is released
@@ -1184,17 +1191,18 @@ void encode_weight_map(CUtensorMap* map, const void* blob_dev, uint32_t blob_byt
 
 void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash, const void* blob_dev,
                        const TcPlan* plan, int mode, const TcJob* jobs, int n_jobs, int kahan, int clamp,
-                       uint32_t* amax, uint32_t* err, cudaStream_t st) {
+                       uint32_t* amax, uint32_t* err, int* tile_ctr, cudaStream_t st) {
   std::string why;
   if (!plan_supported(d, &why)) fail(NWPRT_UNSUPPORTED, why);
   if (n_jobs <= 0) return;
   if (mode == kTcFp8 && !plan) fail(NWPRT_NOT_READY, "FP8 relight without a calibrated plan");
   if (!plan) fail(NWPRT_NOT_READY, "tensor-core relight without packed weights");
   if (mode == kTcCalibrate && !amax) fail(NWPRT_INVALID_ARG, "calibration needs an amax buffer");
+  if (!tile_ctr) fail(NWPRT_INVALID_ARG, "tensor-core relight needs a tile counter");
   if (n_jobs > kInlineJobs) {
     for (int j0 = 0; j0 < n_jobs; j0 += kInlineJobs)
       launch_relight_tc(d, hl, hash, blob_dev, plan, mode, jobs + j0, std::min(kInlineJobs, n_jobs - j0), kahan,
-                        clamp, amax, err, st);
+                        clamp, amax, err, tile_ctr, st);
     return;
   }
   const TcPlan& P = *plan;
@@ -1215,12 +1223,16 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.cp_scale = P.cp_scale;
   p.amax = amax;
   p.err = err;
-  // tile prefix over the jobs
+  // tile prefix over the jobs, longest tiles (largest K) first: the warpgroups take tiles in
+  // this order, so the cheap ones fill the end of the launch
+  int order[kInlineJobs];
+  for (int i = 0; i < n_jobs; ++i) order[i] = i;
+  std::stable_sort(order, order + n_jobs, [&](int a, int b) { return jobs[a].K > jobs[b].K; });
   long long tiles = 0;
   for (int i = 0; i < n_jobs; ++i) {
-    p.jobs[i] = jobs[i];
+    p.jobs[i] = jobs[order[i]];
     p.jobs[i].tile_begin = tiles;
-    tiles += (jobs[i].n_px - jobs[i].px_begin + kTile - 1) / kTile;
+    tiles += (p.jobs[i].n_px - p.jobs[i].px_begin + kTile - 1) / kTile;
   }
   if (tiles == 0) return;
   p.total_tiles = tiles;
@@ -1232,8 +1244,10 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   if (smem > (size_t)max_smem) fail(NWPRT_UNSUPPORTED, "tensor-core relight: shared memory budget exceeded");
   const long long groups = (tiles + kNWG - 1) / kNWG;
   const int grid = (int)(groups < sms ? groups : sms);
+  p.tile_ctr = tile_ctr;
   auto go = [&](auto kern) {
     NWPRT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    NWPRT_CUDA(cudaMemsetAsync(tile_ctr, 0, sizeof(int), st));
     kern<<<grid, kThreads, smem, st>>>(p);
   };
   const int shape = shape_of(P, d);

@@ -283,7 +283,12 @@ class RelightServer:
         ind = torch.empty((fr.width * fr.height, 4), dtype=torch.float32, device=fr.fbPredictedIndirect.device)
         wd = torch.empty_like(ind)
         if r.env_kind == "new":
-            faces = torch.from_numpy(np.ascontiguousarray(r.faces, np.float32)).to(ind.device, non_blocking=True)
+            host = torch.from_numpy(np.ascontiguousarray(r.faces, np.float32))
+            if self.on_gpu:
+                # through pinned memory: a copy from pageable memory may wait for the stream,
+                # i.e. for the launches already queued
+                host = torch.empty(host.shape, dtype=torch.float32, pin_memory=True).copy_(host)
+            faces = host.to(ind.device, non_blocking=True)
         elif r.env_kind == "rot":
             from .engine import env_rotate
             faces = env_rotate(self.base_faces[r.base_env], r.R)
