@@ -258,3 +258,33 @@ def test_dispatcher_on_one_gpu(rig):
     for r in summ["local"]:
         ind, _ = _solo(e, frames, base, r)
         assert torch.equal(r.outputs[0], ind), r.rid
+
+
+def test_env_slots_are_reused_and_grown(rig):
+    """Env slots hold 1,024 wavelets and are reused in stream order; a table larger than every
+    released slot gets a new one (no device-wide synchronisation).  Tables registered in any
+    order read back intact, and the grown slots relight as the FP32 oracle does."""
+    import torch
+    e, frames, base = rig
+    eng = _eng()
+    desc = netconfig.parse(netconfig.CONFIG_LARGE)
+    w = synth.make_weights(desc, seed=0, hash_scale=0.5, param_round="fp16")
+    b = O.Bound(desc, w, synth.make_gbuffer(64, 48, seed=50, flag_prob=0.9))
+    g = np.random.default_rng(9)
+    n, px = 64 * 48, 128
+    for K in (64, 1024, 1500, 16, 2000, 300):
+        idx = g.choice(desc.n_coeffs, K, replace=False).astype(np.int32)
+        st = g.lognormal(0.0, 1.0, size=(K, 3)).astype(np.float32)
+        env = e.addEnvironmentMap(eng.EnvironmentMap(top_coefficients=idx, top_strength=st))
+        gi, gs = e.envWavelets(env)
+        assert np.array_equal(gi, idx) and np.array_equal(gs, st), K
+        if K > 1024:
+            out, out2 = torch.zeros((n, 4), device="cuda"), torch.zeros((n, 4), device="cuda")
+            e.relightRanges([(env, 0, out, out2, 0, px)], eng.RenderConfig(precision="fp32"))
+            e.TCNNSync()
+            ref, _ = O.relight_f32(b, idx, st, px_begin=0, px_end=px)
+            got = out[:px, :3].cpu().numpy()
+            r = ref[:px, :3]
+            rel = np.abs(got - r) / np.maximum(np.abs(r), 1e-6 * np.abs(r).max())
+            assert float(rel.max()) <= 1e-5, (K, float(rel.max()))
+        e.releaseEnvironmentMap(env)
