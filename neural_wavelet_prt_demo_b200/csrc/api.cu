@@ -53,6 +53,7 @@ struct EnvEntry {
   float* strength = nullptr;
   float* emb_k = nullptr;     // [K][D], valid when emb_ready; then [cap][D/2] BF16 pairs
   bool emb_ready = false;
+  bool owned = false;         // buffers of its own (else carved from a chunk of slots)
 };
 
 // The BF16 pairs of an env's embedding rows, stored after the FP32 rows.
@@ -61,9 +62,11 @@ const uint32_t* emb_pairs(const EnvEntry& e, int D) {
 }
 
 void free_env_buffers(EnvEntry& e) {
-  dev_free(e.idx);
-  dev_free(e.strength);
-  dev_free(e.emb_k);
+  if (e.owned) {
+    dev_free(e.idx);
+    dev_free(e.strength);
+    dev_free(e.emb_k);
+  }
   e = EnvEntry{};
 }
 
@@ -100,6 +103,7 @@ struct nwprt_ctx {
   bool fp8_ready = false;
   std::vector<float> fp8_amax;
   std::vector<EnvEntry> envs;
+  std::vector<void*> env_chunks;  // device memory the pooled env slots are carved from
   Frame frames[NWPRT_MAX_FRAMES];
   uint32_t* d_err = nullptr;
   // Tile counters of the tensor-core relight (its warpgroups take tiles from one counter per
@@ -122,6 +126,7 @@ struct nwprt_ctx {
     dev_free(d_tile_ctr);
     dev_free(d_stage);
     for (auto& e : envs) free_env_buffers(e);
+    for (void* c : env_chunks) dev_free(c);
     for (auto& f : frames) dev_free(f.packed);
   }
 };
@@ -194,12 +199,17 @@ void ensure_emb(nwprt_ctx* ctx, EnvEntry& e, cudaStream_t st) {
 }
 
 // Registers an env slot for K wavelets.  Released slots are reused in stream order without
-// any allocation or synchronisation: a slot holds kEnvSlotWavelets wavelets (or K, if larger;
-// ~200 KB at 32 hash features), so any released slot fits any K the Haar path produces.  A K
-// that no released slot fits gets a new slot; slots are freed with the context.  (Replacing a
-// smaller slot would need a device-wide synchronisation before its buffers could be freed,
-// which drains a serving loop's queue of launches.)
+// any allocation or synchronisation: a pooled slot holds kEnvSlotWavelets wavelets (~200 KB at
+// 32 hash features), so any released slot fits any K the Haar path produces.  Pooled slots come
+// kEnvChunkSlots at a time from one allocation, since a serving loop's live set can grow to
+// hundreds of env maps and each cudaMalloc costs milliseconds of host time.  A larger K gets a
+// slot with buffers of its own.  Slots are freed with the context.  (Replacing a smaller slot
+// would need a device-wide synchronisation before its buffers could be freed, which drains a
+// serving loop's queue of launches.)
 constexpr int kEnvSlotWavelets = 1024;
+constexpr int kEnvChunkSlots = 64;
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 int new_env(nwprt_ctx* ctx, int K, int D) {
   int id = -1;
@@ -208,18 +218,34 @@ int new_env(nwprt_ctx* ctx, int K, int D) {
     if (e.live || e.cap < K) continue;
     if (id < 0 || e.cap < ctx->envs[id].cap) id = (int)i;
   }
-  if (id < 0) {
-    const int cap = std::max(K, kEnvSlotWavelets);
+  if (id < 0 && K <= kEnvSlotWavelets) {
+    const size_t cap = kEnvSlotWavelets;
+    const size_t b_idx = align256(cap * 4), b_st = align256(cap * 12), b_emb = align256(cap * (D + D / 2) * 4);
+    const size_t per = b_idx + b_st + b_emb;
+    uint8_t* base = dev_alloc<uint8_t>(per * kEnvChunkSlots);
+    ctx->env_chunks.push_back(base);
+    id = (int)ctx->envs.size();
+    for (int j = 0; j < kEnvChunkSlots; ++j) {
+      EnvEntry e;
+      uint8_t* p = base + per * j;
+      e.idx = reinterpret_cast<int32_t*>(p);
+      e.strength = reinterpret_cast<float*>(p + b_idx);
+      e.emb_k = reinterpret_cast<float*>(p + b_idx + b_st);
+      e.cap = (int)cap;
+      ctx->envs.push_back(e);
+    }
+  } else if (id < 0) {
     EnvEntry e;
+    e.owned = true;
     try {
-      e.idx = dev_alloc<int32_t>(cap);
-      e.strength = dev_alloc<float>((size_t)cap * 3);
-      e.emb_k = dev_alloc<float>((size_t)cap * D + (size_t)cap * (D / 2));
+      e.idx = dev_alloc<int32_t>(K);
+      e.strength = dev_alloc<float>((size_t)K * 3);
+      e.emb_k = dev_alloc<float>((size_t)K * D + (size_t)K * (D / 2));
     } catch (...) {
       free_env_buffers(e);
       throw;
     }
-    e.cap = cap;
+    e.cap = K;
     ctx->envs.push_back(e);
     id = (int)ctx->envs.size() - 1;
   }

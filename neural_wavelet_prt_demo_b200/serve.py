@@ -359,6 +359,9 @@ class RelightServer:
         now = lambda: time.perf_counter() - t0
         finished = 0
         total = len(requests)
+        busy_ms = 0.0  # device time of the relight launches
+        host = {"admit": 0.0, "plan": 0.0, "launch": 0.0, "wait": 0.0}  # host seconds per phase
+        starved = 0  # launches issued with nothing left queued on the GPU
         # transfers of refused or failed bands may still be queued once every request has
         # ended here: the loop runs until the completion has nothing outstanding either
         while finished < total or self.completion.outstanding():
@@ -376,6 +379,7 @@ class RelightServer:
                 r.status = "queued"
                 queue.append(r)
             # admission (FCFS under the byte budget; over-budget and stale requests are refused)
+            t_ph = time.perf_counter()
             while queue and (self.max_active_cap is None or len(active) < self.max_active_cap):
                 r = queue[0]
                 try:
@@ -414,8 +418,11 @@ class RelightServer:
                 self.completion.admitted(r)
                 active.append(r)
             self.max_active = max(self.max_active, len(active))
+            host["admit"] += time.perf_counter() - t_ph
             if active and len(in_flight) < self.max_in_flight:
+                t_ph = time.perf_counter()
                 plan = plan_quantum(active, self.quantum, self.order, self.rate)
+                host["plan"] += time.perf_counter() - t_ph
                 launch = []
                 for r, b, e in plan:
                     try:
@@ -429,8 +436,15 @@ class RelightServer:
                     launch.append((r, (r.env_id, r.res, r.outputs[0], r.outputs[1], b, e), e))
                 if not launch:
                     continue
+                t_ph = time.perf_counter()
                 if self.on_gpu:
                     torch.cuda.nvtx.range_push(f"quantum {self.quanta}: {len(launch)} requests")
+                    ev0 = torch.cuda.Event(enable_timing=True)
+                    ev0.record(self.stream)
+                    if self.quanta and (not in_flight or in_flight[-1][1].query()):
+                        starved += 1
+                else:
+                    ev0 = None
                 failed = self._launch([(r, rg) for r, rg, _ in launch])
                 if self.on_gpu:
                     torch.cuda.nvtx.range_pop()
@@ -441,17 +455,22 @@ class RelightServer:
                 for r, _, e in launch:
                     if r.status == "active":
                         r.next_px = e
-                ev = torch.cuda.Event() if self.on_gpu else _HostEvent()
+                ev = torch.cuda.Event(enable_timing=True) if self.on_gpu else _HostEvent()
                 ev.record(self.stream)
                 done_now = [r for r, _, _ in launch if r.status == "active" and r.next_px >= r.n_px]
                 for r in done_now:
                     active.remove(r)
-                in_flight.append((ev, done_now))
+                in_flight.append((ev0, ev, done_now))
                 self.quanta += 1
+                host["launch"] += time.perf_counter() - t_ph
                 continue
             if in_flight:
-                ev, done_now = in_flight.popleft()
+                ev0, ev, done_now = in_flight.popleft()
+                t_ph = time.perf_counter()
                 ev.synchronize()
+                host["wait"] += time.perf_counter() - t_ph
+                if ev0 is not None:
+                    busy_ms += ev0.elapsed_time(ev)
                 t = now()
                 for r in done_now:
                     if self.completion.finished(r):
@@ -472,7 +491,13 @@ class RelightServer:
             if queue:  # nothing active, nothing in flight, but the head does not fit: cannot happen
                 raise RuntimeError("admission stalled")
         self.e.TCNNSync()
-        return summarize(requests, now())
+        out = summarize(requests, now())
+        if self.on_gpu and out["makespan_s"] > 0:
+            # share of the run the GPU spent in relight launches (the rest: idle or env set-up)
+            out["relight_busy_frac"] = busy_ms / 1e3 / out["makespan_s"]
+            out["host_s"] = {k: round(v, 3) for k, v in host.items()}
+            out["launches_after_idle"] = starved
+        return out
 
 
 # latency classes of the serving stream: resolutions up to 1280x720, and larger ones
