@@ -179,7 +179,9 @@ NWPRT_API nwprt_status nwprt_prepare(nwprt_ctx* ctx, int frame_id, const nwprt_g
  * N x K transport never reaches memory).  Replaces RenderEngine::TCNNPass_p2
  * (tinycudann/tcnn.cu:111-152), PRT_Network::inference (prt_network.h:73-154) and
  * prt::computeResponse (utils_kernels.h:52-91).  Asynchronous: unlike the reference it
- * does not block the host.  `opts` NULL = {FP32, clamp, kahan}. */
+ * does not block the host.  `opts` NULL = {FP32, clamp, kahan}.  BF16/FP8 relights may be
+ * captured into a CUDA graph: each captured launch keeps one of the context's 64 tile
+ * counters for good (a further capture fails with NWPRT_UNSUPPORTED). */
 NWPRT_API nwprt_status nwprt_relight(nwprt_ctx* ctx, int env_id, int frame_id,
                            const nwprt_relight_opts* opts, float* indirect, float* with_direct,
                            void* stream);

@@ -107,10 +107,12 @@ struct nwprt_ctx {
   Frame frames[NWPRT_MAX_FRAMES];
   uint32_t* d_err = nullptr;
   // Tile counters of the tensor-core relight (its warpgroups take tiles from one counter per
-  // launch): a ring, so that launches in flight on different streams use different counters.
-  static constexpr int kTileCounters = 64;
+  // launch): a ring for eager launches, so that launches in flight on different streams use
+  // different counters, and one counter of its own for each launch captured into a CUDA graph
+  // (a graph replays its counter, so no later launch may be handed it).
+  static constexpr int kTileCounters = 64, kCapturedCounters = 64;
   int* d_tile_ctr = nullptr;
-  int tile_ctr_next = 0;
+  int tile_ctr_next = 0, captured_next = 0;
   float* d_stage = nullptr;
   size_t stage_cap = 0;
 
@@ -319,7 +321,7 @@ nwprt_status nwprt_create(const char* config_json, int device, nwprt_ctx** out) 
     c->tc_supported = relight_tc_supported(d, &c->tc_why);
     c->d_err = dev_alloc<uint32_t>(1);
     NWPRT_CUDA(cudaMemset(c->d_err, 0, sizeof(uint32_t)));
-    c->d_tile_ctr = dev_alloc<int>(nwprt_ctx::kTileCounters);
+    c->d_tile_ctr = dev_alloc<int>(nwprt_ctx::kTileCounters + nwprt_ctx::kCapturedCounters);
     *out = c.release();
   });
 }
@@ -602,8 +604,17 @@ static void relight_many_tc(nwprt_ctx* ctx, const RangeReq* reqs, int n_reqs, co
                          0, r.px_begin, emb_pairs(e, ctx->dims.enc_dims())});
   }
   if (jobs.empty()) return;
-  int* ctr = ctx->d_tile_ctr + ctx->tile_ctr_next;
-  ctx->tile_ctr_next = (ctx->tile_ctr_next + 1) % nwprt_ctx::kTileCounters;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  NWPRT_CUDA(cudaStreamIsCapturing(st, &cs));
+  int* ctr;
+  if (cs == cudaStreamCaptureStatusActive) {
+    need(ctx->captured_next < nwprt_ctx::kCapturedCounters, NWPRT_UNSUPPORTED,
+         "too many tensor-core relights captured into CUDA graphs for one context (64)");
+    ctr = ctx->d_tile_ctr + nwprt_ctx::kTileCounters + ctx->captured_next++;
+  } else {
+    ctr = ctx->d_tile_ctr + ctx->tile_ctr_next;
+    ctx->tile_ctr_next = (ctx->tile_ctr_next + 1) % nwprt_ctx::kTileCounters;
+  }
   if (mode == kTcFp8)
     launch_relight_tc(ctx->dims, ctx->hl, ctx->d_hash, ctx->d_tc_w8, &ctx->fp8_plan, mode, jobs.data(),
                       (int)jobs.size(), o.kahan, o.clamp_terms, nullptr, ctx->d_err, ctr, st);
