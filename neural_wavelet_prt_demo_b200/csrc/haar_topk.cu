@@ -1,4 +1,6 @@
-// Cubemap Haar transform + top-K wavelet selection, one thread-block cluster per env map.
+// Cubemap Haar transform + top-K wavelet selection: one thread-block cluster per env map for
+// single maps and small batches, one persistent CTA per map for batches of 32 maps or more
+// (haar_topk_batch_kernel, described where it is defined).
 //
 // The reference only loads precomputed results (waveletcoeffs/<name>.npy and
 // waveletstrength/<name>.npy, Renderer/EnvironmentMap.cpp:97-108); the transform and
@@ -9,8 +11,8 @@
 //  * key = |0.212671 r + 0.715160 g + 0.072169 b| (EnvironmentMap.cpp:149-151), NaN -> 0;
 //  * order = key descending, flat index face*S*S + row*S + col ascending.
 //
-// Design: a cluster of 6 CTAs (one per face) of 256 threads.  Nothing but the inputs and
-// outputs touches global memory, and the face never goes through shared memory:
+// Cluster form: 6 CTAs (one per face) of 256 threads.  Nothing but the inputs and outputs
+// touches global memory, and the face never goes through shared memory:
 //  * Haar in registers.  Thread t owns the 4x4 texel block at block coordinates
 //    (bi, bj) = Morton(t) (bj on the even bits) and evaluates the first two levels on it
 //    alone: 15 detail coefficients stay in its registers, one LL value moves on.  Because
@@ -538,9 +540,13 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
 // only each thread's upper-block entry is kept, in this CTA's slice of a global scratch
 // buffer ([face][channel][thread], 18 KB at S = 64, so it stays in L2); the K winners' other
 // coefficients are recomputed from their texel blocks (block_coef), which costs far less
-// than writing and re-reading all 6 * S * S of them.  The select is the cluster form's,
-// block-local: per-warp histograms, a bitmap of ties over the 6*S*S flat indices, winner
-// slots from one block scan, and a rank by broadcast reads of the K keys.
+// than writing and re-reading all 6 * S * S of them.  The select is block-local: a first
+// histogram pass over a window of 16 binades below the map's largest key; when that finds the
+// K-th largest key's bin, one scan sorts the keys above it (winners) from those in it
+// (candidates, ranked directly); otherwise radix passes, a bitmap of ties over the 6*S*S flat
+// indices and winner slots from one block scan.  The winners are ordered by a counting pass
+// over their key range.  Faces alternate between two `upper` buffers, so they need no block
+// barrier of their own.
 
 struct BatchSmem {
   uint4* keys;      // [6][NK/4][kThreads]
