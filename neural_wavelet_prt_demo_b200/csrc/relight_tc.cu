@@ -19,8 +19,9 @@
 // kernel shared-memory-bandwidth bound (operand reads + epilogue stores ~266 KB per tile and
 // wavelet).  So activations live in TMEM: the A operand of every layer is read by the MMA
 // straight from tensor memory (the ".kind::f16 [d], [a], b_desc" form), and the epilogue
-// writes it back with a single tcgen05.st.  Only the weights (B) and the per-tile aux block
-// come from shared memory; V_last, the FP32 output layer, comes from the kernel parameters.
+// writes it back with a single tcgen05.st.  Only the weights (B, loaded once per CTA by TMA)
+// and the per-tile aux block come from shared memory; the FP32-dot forms take V_last, the
+// output layer, from the kernel parameters.
 //
 // Organisation (one persistent CTA per SM): kNWG = 5 warpgroups, one 128-pixel tile each,
 // 96 TMEM columns per tile (480 of 512): [0,32) the BF16 A operand (2 values per 32-bit
@@ -32,9 +33,12 @@
 // layer: wait on the tile's commit barrier -> tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 ->
 // tcgen05.st into the A columns -> warpgroup barrier (bar.red.and carrying the "no
 // timeout" vote) -> an elected lane of warp 0 issues the next layer's MMAs and commits
-// them.  The output layer's epilogue (or, in the FP32-dot forms, the last
-// hidden layer's) forms T_k, does the clamped Kahan sum and writes the next wavelet's
-// first-layer operand hash(p) * E_k+1.  The two standard networks run
+// them.  In the BF16 fixed-sequence kernels the last hidden layer's FP16 operand goes to
+// accumulator columns [64, 96), the next wavelet's first-layer operand hash(p) * E_k+1 is
+// written into the A columns while the output MMA runs, and T_k's clamped Kahan sum is formed
+// after the hand-off to that next wavelet; the FP32-dot forms do all three in the last hidden
+// layer's epilogue.  Warpgroups take tiles from a per-launch counter, so tiles of different
+// cost (requests of different K) balance across the SMs.  The two standard networks run
 // kernels specialised on their layer sequence (ShapeOf), every other supported network a
 // generic form that reads the sequence from the plan.  Every wait is bounded by
 // %globaltimer (2 s); on expiry the kernel records kDevWaitTimeout and the warpgroup
