@@ -62,6 +62,9 @@ def parse_args():
                          "request size, arrival, or least remaining work)")
     ap.add_argument("--serve-max-active", type=int, default=0,
                     help="serve: admit at most this many requests at once (0: the byte budget alone)")
+    ap.add_argument("--serve-in-flight", type=int, default=2,
+                    help="serve: relight launches kept queued on the GPU (1: a new request waits behind at "
+                         "most one quantum, at the cost of a gap between launches)")
     ap.add_argument("--serve-serial-prefix", type=int, default=40,
                     help="requests of the stream also served by the plain FP32 serial baseline")
     ap.add_argument("--fp8-steps", type=int, default=5, help="timed steps of the FP8 form (0: skip)")
@@ -793,7 +796,8 @@ def run_serve(args, rank, world, local, dev):
             rate = float(t.item())
         reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=0, face_size=S)
         kw = dict(precision="bf16", budget_bytes=150 << 30, quantum_ms=args.serve_quantum_ms, est_evals_per_s=rate,
-                  max_active=args.serve_max_active or None, order=args.serve_order)
+                  max_active=args.serve_max_active or None, order=args.serve_order,
+                  max_in_flight=max(1, args.serve_in_flight))
         frame_px = [f.width * f.height for f in frames]
         first = clocks is None
         if first:
