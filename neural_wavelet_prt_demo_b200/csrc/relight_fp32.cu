@@ -87,6 +87,21 @@ __device__ __forceinline__ void hash_encode(const HashLevels& hl, const float* _
   }
 }
 
+// Two FP32 values in one 64-bit register, and the packed FMA of sm_100 on such pairs:
+// fma.rn.f32x2 rounds each lane once, exactly as fmaf does, so a pair of output neurons
+// accumulated side by side keeps the oracle's bits with half the FMA instructions.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void f2_fma(unsigned long long& acc, unsigned long long a, unsigned long long b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
+
 // y = act(W x) over one thread's activation column.
 // MODE 0: x_i = act row i.  MODE 1: x_i = act row (ENC + i) * e[i] (the CP product).
 // MODE 2: x_i = act row i for i < OPO, else act row (AUX + i - OPO) (the [out_prd || aux] concat).
@@ -94,25 +109,27 @@ template <int IN, int OUT, bool RELU, int MODE, int NT, int ENC, int AUX, int OP
 __device__ __forceinline__ void dense(const float* __restrict__ Wt, float* act,
                                       const float* __restrict__ e, float* outv) {
   constexpr int O4 = r4(OUT) / 4;
-  float acc[O4 * 4];
+  unsigned long long acc2[O4 * 2];  // output pairs (2j, 2j + 1)
 #pragma unroll
-  for (int j = 0; j < O4 * 4; ++j) acc[j] = 0.f;
+  for (int j = 0; j < O4 * 2; ++j) acc2[j] = 0ull;
 #pragma unroll 4
   for (int i = 0; i < IN; ++i) {
     float xi;
     if (MODE == 0) xi = act[i * NT];
     else if (MODE == 1) xi = __fmul_rn(act[(ENC + i) * NT], e[i]);
     else xi = (i < OPO) ? act[i * NT] : act[(AUX + i - OPO) * NT];
+    const unsigned long long x2 = f2_pack(xi, xi);
     const float4* w4 = reinterpret_cast<const float4*>(Wt + i * O4 * 4);
 #pragma unroll
     for (int j = 0; j < O4; ++j) {
       const float4 w = w4[j];
-      acc[4 * j + 0] = fmaf(w.x, xi, acc[4 * j + 0]);
-      acc[4 * j + 1] = fmaf(w.y, xi, acc[4 * j + 1]);
-      acc[4 * j + 2] = fmaf(w.z, xi, acc[4 * j + 2]);
-      acc[4 * j + 3] = fmaf(w.w, xi, acc[4 * j + 3]);
+      f2_fma(acc2[2 * j], f2_pack(w.x, w.y), x2);
+      f2_fma(acc2[2 * j + 1], f2_pack(w.z, w.w), x2);
     }
   }
+  float acc[O4 * 4];
+#pragma unroll
+  for (int j = 0; j < O4 * 2; ++j) f2_unpack(acc2[j], acc[2 * j], acc[2 * j + 1]);
 #pragma unroll
   for (int j = 0; j < OUT; ++j) {
     const float v = RELU ? fmaxf(acc[j], 0.f) : acc[j];
@@ -249,27 +266,29 @@ struct GenNet {
 template <int NT>
 __device__ __forceinline__ void dense_rt(const GenLayer& L, const GenNet& g, const float* __restrict__ Wt,
                                          float* act, const float* __restrict__ e, float* outv) {
-  float acc[kGenMaxOut];
+  unsigned long long acc2[kGenMaxOut / 2];  // output pairs (2j, 2j + 1)
 #pragma unroll
-  for (int j = 0; j < kGenMaxOut; ++j) acc[j] = 0.f;
+  for (int j = 0; j < kGenMaxOut / 2; ++j) acc2[j] = 0ull;
   const int o4 = (L.out + 3) / 4;
   for (int i = 0; i < L.in; ++i) {
     float xi;
     if (L.mode == 0) xi = act[i * NT];
     else if (L.mode == 1) xi = __fmul_rn(act[(g.enc + i) * NT], e[i]);
     else xi = (i < g.opo) ? act[i * NT] : act[(g.aux + i - g.opo) * NT];
+    const unsigned long long x2 = f2_pack(xi, xi);
     const float4* w4 = reinterpret_cast<const float4*>(Wt + (size_t)i * o4 * 4);
 #pragma unroll
     for (int j = 0; j < kGenMaxOut / 4; ++j) {
       if (j < o4) {
         const float4 w = w4[j];
-        acc[4 * j + 0] = fmaf(w.x, xi, acc[4 * j + 0]);
-        acc[4 * j + 1] = fmaf(w.y, xi, acc[4 * j + 1]);
-        acc[4 * j + 2] = fmaf(w.z, xi, acc[4 * j + 2]);
-        acc[4 * j + 3] = fmaf(w.w, xi, acc[4 * j + 3]);
+        f2_fma(acc2[2 * j], f2_pack(w.x, w.y), x2);
+        f2_fma(acc2[2 * j + 1], f2_pack(w.z, w.w), x2);
       }
     }
   }
+  float acc[kGenMaxOut];
+#pragma unroll
+  for (int j = 0; j < kGenMaxOut / 2; ++j) f2_unpack(acc2[j], acc[2 * j], acc[2 * j + 1]);
 #pragma unroll
   for (int j = 0; j < kGenMaxOut; ++j) {
     if (j < L.out) {
