@@ -227,7 +227,10 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
-        dist.init_process_group("nccl", device_id=dev)
+        # a short timeout: ranks waiting on a failed peer end with an error instead of hanging
+        # (the longest stretch without a collective is a rank-0 host phase of ~20 s)
+        import datetime
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=300))
 
     if args.workload == "sh1080":
         return run_sh(args, rank, world, local, dev)
