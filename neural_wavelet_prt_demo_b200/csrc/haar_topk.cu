@@ -373,7 +373,9 @@ __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__
 }
 
 template <int S>
-__global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 3)
+// Two CTAs per SM at most: this form serves batches under kBatchMinMaps (at most 186 CTAs
+// on 148 SMs), and the bound leaves the transform its registers (three per SM spilled).
+__global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 2)
     haar_topk_kernel(const float* __restrict__ faces, int K, int32_t* __restrict__ idx_out,
                      float* __restrict__ st_out) {
   using F = FaceGeom<S>;
