@@ -181,6 +181,31 @@ __device__ __forceinline__ void shuffle_level(float ll[3], int lane, int s, int 
   }
 }
 
+// shuffle_level with the details stored to a face's scratch slice, laid out [channel][thread]
+// (thread i * G + j owns upper-block entry (i, j)).
+__device__ __forceinline__ void shuffle_level_scratch(float ll[3], int lane, int s, int m, int h, bool live,
+                                                      float* upf, int G) {
+  float v[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    v[0][c] = __shfl_down_sync(0xffffffffu, ll[c], s);
+    v[1][c] = __shfl_down_sync(0xffffffffu, ll[c], 2 * s);
+    v[2][c] = __shfl_down_sync(0xffffffffu, ll[c], 3 * s);
+  }
+  if (live && (lane & (4 * s - 1)) == 0) {
+    const int j = morton_even(m), i = morton_even(m >> 1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float a, hl, lh, hh;
+      haar4(ll[c], v[0][c], v[1][c], v[2][c], a, hl, lh, hh);
+      ll[c] = a;
+      upf[c * 256 + i * G + j + h] = hl;
+      upf[c * 256 + (i + h) * G + j] = lh;
+      upf[c * 256 + (i + h) * G + j + h] = hh;
+    }
+  }
+}
+
 // Geometry of one face's transform: thread t < T owns the B x B texel block at Morton(t).
 template <int S>
 struct FaceGeom {
@@ -238,92 +263,115 @@ __device__ __forceinline__ void block_coef(const float* __restrict__ src, int ti
   }
 }
 
+// The first part of the transform below, split out for the batched form: block_load loads
+// thread t's B x B texel block (t < T), block_levels runs levels 1-2 on it in registers (co:
+// its NR detail coefficients, ll: the block's LL value), with the same operations in the same
+// order as haar_face_in_registers.
+template <int S>
+__device__ __forceinline__ void block_load(const float* __restrict__ src, int tid,
+                                           float (&px)[FaceGeom<S>::B][FaceGeom<S>::B][3]) {
+  using F = FaceGeom<S>;
+  constexpr int B = F::B;
+  if (tid >= F::T) return;
+  const int bj = morton_even(tid), bi = morton_even(tid >> 1);
+  const float* blk = src + ((size_t)(B * bi) * S + B * bj) * 3;
+  if constexpr (B == 4) {
+    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const float4* row = reinterpret_cast<const float4*>(blk + (size_t)r * S * 3);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float4 v = __ldg(row + q);
+          const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int k = 0; k < 4; ++k) px[r][(4 * q + k) / 3][(4 * q + k) % 3] = e[k];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 12; ++q) px[r][q / 3][q % 3] = __ldg(blk + (size_t)r * S * 3 + q);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+#pragma unroll
+      for (int q = 0; q < 3 * B; ++q) px[r][q / 3][q % 3] = __ldg(blk + (size_t)r * S * 3 + q);
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void block_levels(const float (&px)[FaceGeom<S>::B][FaceGeom<S>::B][3], int tid,
+                                             float (&co)[FaceGeom<S>::NR > 0 ? FaceGeom<S>::NR : 1][3],
+                                             float (&ll)[3]) {
+  using F = FaceGeom<S>;
+  constexpr int B = F::B, NR = F::NR;
+#pragma unroll
+  for (int u = 0; u < (NR > 0 ? NR : 1); ++u) co[u][0] = co[u][1] = co[u][2] = 0.f;
+  ll[0] = ll[1] = ll[2] = 0.f;
+  if (tid >= F::T) return;
+  if constexpr (B == 4) {
+    float l1[2][2][3];
+#pragma unroll
+    for (int qi = 0; qi < 2; ++qi)
+#pragma unroll
+      for (int qj = 0; qj < 2; ++qj)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float a, hl, lh, hh;
+          haar4(px[2 * qi][2 * qj][c], px[2 * qi][2 * qj + 1][c], px[2 * qi + 1][2 * qj][c],
+                px[2 * qi + 1][2 * qj + 1][c], a, hl, lh, hh);
+          l1[qi][qj][c] = a;
+          const int u = (qi * 2 + qj) * 3;
+          co[u][c] = hl;
+          co[u + 1][c] = lh;
+          co[u + 2][c] = hh;
+        }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float a, hl, lh, hh;
+      haar4(l1[0][0][c], l1[0][1][c], l1[1][0][c], l1[1][1][c], a, hl, lh, hh);
+      ll[c] = a;
+      co[12][c] = hl;
+      co[13][c] = lh;
+      co[14][c] = hh;
+    }
+  } else if constexpr (B == 2) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float a, hl, lh, hh;
+      haar4(px[0][0][c], px[0][1][c], px[1][0][c], px[1][1][c], a, hl, lh, hh);
+      ll[c] = a;
+      co[0][c] = hl;
+      co[1][c] = lh;
+      co[2][c] = hh;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ll[c] = px[0][0][c];
+  }
+}
+
 // The full Haar transform of one face [S][S][3] at `src` by the block's kThreads threads:
 // levels 1-2 on each thread's B x B block in registers (co: its NR detail coefficients),
 // the next levels by warp shuffles, the last ones in warp 0.  The G x G upper block of the
 // result (levels >= 3 and the DC term) lands in `upper` [G*G][3]; `llg` is [16][3] staging.
-// Ends with a block barrier, after which `upper` is complete.  PARTIAL_TAIL (for S >= 32, where
-// the last levels run in warp 0 after a block barrier): only the warps whose own upper-block
-// entries those levels write wait for them, on a named barrier; every other entry was written
-// before the block barrier.  The caller then alternates `upper` and `llg` between two buffers.
-template <int S, bool PARTIAL_TAIL = false>
+// Ends with a block barrier, after which `upper` is complete.
+template <int S>
 __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__ src, int tid,
                                                        float (&co)[FaceGeom<S>::NR > 0 ? FaceGeom<S>::NR : 1][3],
                                                        float* upper, float* llg) {
   using F = FaceGeom<S>;
-  constexpr int B = F::B, G = F::G, T = F::T, NR = F::NR;
+  constexpr int G = F::G;
   const int lane = tid & 31, warp = tid >> 5;
-  const bool owner = tid < T;
-  const int bj = morton_even(tid), bi = morton_even(tid >> 1);
-  // ---- levels 1 and 2 on this thread's B x B block, in registers
-#pragma unroll
-  for (int u = 0; u < (NR > 0 ? NR : 1); ++u) co[u][0] = co[u][1] = co[u][2] = 0.f;
-  float ll[3] = {0.f, 0.f, 0.f};
-  if (owner) {
-    float px[B][B][3];
-    const float* blk = src + ((size_t)(B * bi) * S + B * bj) * 3;
-    if constexpr (B == 4) {
-      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const float4* row = reinterpret_cast<const float4*>(blk + (size_t)r * S * 3);
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            const float4 v = __ldg(row + q);
-            const float e[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) px[r][(4 * q + k) / 3][(4 * q + k) % 3] = e[k];
-          }
-        }
-      } else {
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int q = 0; q < 12; ++q) px[r][q / 3][q % 3] = __ldg(blk + (size_t)r * S * 3 + q);
-      }
-      float l1[2][2][3];
-#pragma unroll
-      for (int qi = 0; qi < 2; ++qi)
-#pragma unroll
-        for (int qj = 0; qj < 2; ++qj)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            float a, hl, lh, hh;
-            haar4(px[2 * qi][2 * qj][c], px[2 * qi][2 * qj + 1][c], px[2 * qi + 1][2 * qj][c],
-                  px[2 * qi + 1][2 * qj + 1][c], a, hl, lh, hh);
-            l1[qi][qj][c] = a;
-            const int u = (qi * 2 + qj) * 3;
-            co[u][c] = hl;
-            co[u + 1][c] = lh;
-            co[u + 2][c] = hh;
-          }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float a, hl, lh, hh;
-        haar4(l1[0][0][c], l1[0][1][c], l1[1][0][c], l1[1][1][c], a, hl, lh, hh);
-        ll[c] = a;
-        co[12][c] = hl;
-        co[13][c] = lh;
-        co[14][c] = hh;
-      }
-    } else if constexpr (B == 2) {
-#pragma unroll
-      for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) px[r][q / 3][q % 3] = __ldg(blk + (size_t)r * S * 3 + q);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float a, hl, lh, hh;
-        haar4(px[0][0][c], px[0][1][c], px[1][0][c], px[1][1][c], a, hl, lh, hh);
-        ll[c] = a;
-        co[0][c] = hl;
-        co[1][c] = lh;
-        co[2][c] = hh;
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) ll[c] = __ldg(src + c);
-    }
+  const bool owner = tid < F::T;
+  float ll[3];
+  {
+    float px[F::B][F::B][3];
+    block_load<S>(src, tid, px);
+    block_levels<S>(px, tid, co, ll);
   }
   // ---- the remaining levels over the G x G LL grid, held in Morton order by threads 0..T-1
   {
@@ -362,14 +410,7 @@ __device__ __forceinline__ void haar_face_in_registers(const float* __restrict__
       for (int c = 0; c < 3; ++c) upper[c] = ll[c];
     }
   }
-  if constexpr (PARTIAL_TAIL && G >= 8) {
-    // warp 0 finished an n x n LL grid, n = G / 4: it wrote entries (i, j), i, j < n, read by
-    // threads i * G + j, i.e. the first NT warps
-    constexpr int n = G / 4, NT = ((n - 1) * G + n - 1) / 32 + 1;
-    if (warp < NT) asm volatile("bar.sync 1, %0;" ::"n"(NT * 32) : "memory");
-  } else {
-    __syncthreads();
-  }
+  __syncthreads();
 }
 
 template <int S>
@@ -547,8 +588,9 @@ __global__ void __cluster_dims__(6, 1, 1) __launch_bounds__(kThreads, 2)
 // K-th largest key's bin, one scan sorts the keys above it (winners) from those in it
 // (candidates, ranked directly); otherwise radix passes, a bitmap of ties over the 6*S*S flat
 // indices and winner slots from one block scan.  The winners are ordered by a counting pass
-// over their key range.  Faces alternate between two `upper` buffers, so they need no block
-// barrier of their own.
+// over their key range.  The faces need no block barrier between them: levels 1-2 are
+// thread-local, levels 3-4 (warp shuffles) write their details straight to the scratch slice,
+// and the last levels of all six faces run after one barrier, in warps 0-5.
 
 struct BatchSmem {
   uint4* keys;      // [6][NK/4][kThreads]
@@ -557,14 +599,12 @@ struct BatchSmem {
   uint32_t* wpre;   // [6*S*S/32]
   uint64_t* gkey;   // [K]
   int* gid;         // [K] winner: (face * NK + u) * kThreads + thread
-  float* upper;     // [(S/4)^2][3]
-  float* llg;       // [2][16][3], alternating by face
+  float* llg;       // [6][16][3] each face's LL values left for its last levels
   int* warp_tot;
   int* scal;
 };
 
 __host__ __device__ inline size_t batch_smem_layout(int S, int K, char* base, BatchSmem* L) {
-  const int G = S < 4 ? 1 : S / 4;
   const int nk = S >= 4 ? 16 : (S == 2 ? 4 : 1);
   const int nkq = (nk + 3) / 4;
   const int nw = (6 * S * S + 31) / 32;
@@ -575,8 +615,7 @@ __host__ __device__ inline size_t batch_smem_layout(int S, int K, char* base, Ba
   const size_t oH = take(uA > uB ? uA : uB);
   const size_t oG = take(sizeof(uint64_t) * K);
   const size_t oI = take(sizeof(int) * K);
-  const size_t oU = take(sizeof(float) * 3 * G * G);
-  const size_t oL = take(sizeof(float) * 3 * 16 * 2);
+  const size_t oL = take(sizeof(float) * 3 * 16 * 6);
   const size_t oW = take(sizeof(int) * kWarps);
   const size_t oS = take(sizeof(int) * 32);
   if (L) {
@@ -586,7 +625,6 @@ __host__ __device__ inline size_t batch_smem_layout(int S, int K, char* base, Ba
     L->wpre = (uint32_t*)(base + oH) + nw;
     L->gkey = (uint64_t*)(base + oG);
     L->gid = (int*)(base + oI);
-    L->upper = (float*)(base + oU);
     L->llg = (float*)(base + oL);
     L->warp_tot = (int*)(base + oW);
     L->scal = (int*)(base + oS);
@@ -609,8 +647,6 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr int NW = (6 * SS + 31) / 32;
   static_assert(T <= kThreads, "one 4x4 block per thread");
   static_assert(kThreads == 256, "one thread per bin of the winners' counting pass");
-  static_assert(3 * FaceGeom<S>::G * FaceGeom<S>::G * sizeof(float) <= kWarps * 256 * sizeof(uint32_t),
-                "the second `upper` buffer fits the histogram region");
   static_assert(512 * sizeof(uint32_t) + kMaxK * sizeof(uint16_t) <= kWarps * 256 * sizeof(uint32_t),
                 "the winners' bins and order fit the histogram region");
   extern __shared__ __align__(16) char smem_raw[];
@@ -622,9 +658,14 @@ __global__ void __launch_bounds__(kThreads, 2)
   float* up = scratch + (size_t)blockIdx.x * batch_scratch_floats_per_cta<S>();
 
   for (int env = blockIdx.x; env < n_env; env += gridDim.x) {
-    // ---- the six transforms: keys to shared memory, upper-block entries to the scratch slice;
-    // each thread keeps the largest key it formed
+    // ---- the six transforms, with no block barrier between faces: levels 1-2 in registers
+    // (their 15 keys straight to shared memory), levels 3-4 by warp shuffles whose details go
+    // to this face's scratch slice, the LL values left over to shared staging.  After all six,
+    // warp f finishes face f's last levels; then every thread reads its own six upper-block
+    // entries and forms their keys.  Each thread keeps the largest key it formed.
     uint32_t kmax = 0;
+    constexpr int G = F::G;
+    constexpr int NL = G >= 8 ? G / 4 : 1;  // side of the LL grid left after levels 3-4
     for (int f = 0; f < 6; ++f) {
       const float* src = faces + ((size_t)env * 6 + f) * (size_t)SS * 3;
       // the next face (after the sixth: this CTA's next map's first) into L2 meanwhile
@@ -634,31 +675,74 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (nxt < (long long)n_env * 6 && (reinterpret_cast<uintptr_t>(pf) & 15) == 0)
           asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(pf), "r"((uint32_t)(SS * 12)) : "memory");
       }
-      // `upper` alternates between two buffers (the second is the histogram region, idle until
-      // the select): a face overwrites only the buffer of the face before last, whose readers
-      // all passed the last face's barriers, so faces need no barrier of their own
-      float* upper = (f & 1) ? reinterpret_cast<float*>(sm.whist) : sm.upper;
-      float co[NR > 0 ? NR : 1][3];
-      haar_face_in_registers<S, true>(src, tid, co, upper, sm.llg + (f & 1) * 48);
+      float* upf = up + f * 3 * kThreads;
       uint32_t k[NKQ * 4];
 #pragma unroll
       for (int u = 0; u < NKQ * 4; ++u) k[u] = 0u;
-      if (owner) {
+      float ll[3];
+      {
+        float px[F::B][F::B][3];
+        float co[NR > 0 ? NR : 1][3];
+        block_load<S>(src, tid, px);
+        block_levels<S>(px, tid, co, ll);
+        if (owner)
 #pragma unroll
-        for (int u = 0; u < NR; ++u) k[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
-        const float ur = upper[tid * 3], ug = upper[tid * 3 + 1], ub = upper[tid * 3 + 2];
-        k[NR] = wavelet_key_bits(ur, ug, ub);
-#pragma unroll
-        for (int u = 0; u <= NR; ++u) kmax = max(kmax, k[u]);
-        up[(f * 3 + 0) * kThreads + tid] = ur;
-        up[(f * 3 + 1) * kThreads + tid] = ug;
-        up[(f * 3 + 2) * kThreads + tid] = ub;
+          for (int u = 0; u < NR; ++u) {
+            k[u] = wavelet_key_bits(co[u][0], co[u][1], co[u][2]);
+            kmax = max(kmax, k[u]);
+          }
       }
 #pragma unroll
       for (int q = 0; q < NKQ; ++q)
         sm.keys[((size_t)f * NKQ + q) * kThreads + tid] = make_uint4(k[4 * q], k[4 * q + 1], k[4 * q + 2], k[4 * q + 3]);
+      int n = G, st_ = 1;
+#pragma unroll
+      for (int lev = 0; lev < 2; ++lev)
+        if (n >= 2) {
+          shuffle_level_scratch(ll, lane, st_, tid / (4 * st_), n / 2, owner, upf, G);
+          n /= 2;
+          st_ *= 4;
+        }
+      if (n >= 2) {
+        if (owner && (tid & (st_ - 1)) == 0)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) sm.llg[(f * 16 + tid / st_) * 3 + c] = ll[c];
+      } else if (tid == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) upf[c * kThreads] = ll[c];  // the DC term
+      }
     }
-    __syncthreads();  // the last face's `upper` (the histogram region) is read; the select reuses it
+    __syncthreads();  // every face's level-3/4 details and LL staging are written
+    if constexpr (NL >= 2) {
+      if (warp < 6) {
+        const int f = warp;
+        float* upf = up + f * 3 * kThreads;
+        const bool live = lane < NL * NL;
+        float ll[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ll[c] = live ? sm.llg[(f * 16 + lane) * 3 + c] : 0.f;
+        int n = NL, s2 = 1;
+#pragma unroll
+        for (int lev = 0; lev < 2; ++lev)
+          if (n >= 2) {
+            shuffle_level_scratch(ll, lane, s2, lane / (4 * s2), n / 2, live, upf, G);
+            n /= 2;
+            s2 *= 4;
+          }
+        if (lane == 0)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) upf[c * kThreads] = ll[c];  // the DC term
+      }
+      __syncthreads();  // the last levels' details are written
+    }
+    if (owner)
+      for (int f = 0; f < 6; ++f) {
+        const float* upf = up + f * 3 * kThreads;
+        const uint32_t kk = wavelet_key_bits(upf[tid], upf[kThreads + tid], upf[2 * kThreads + tid]);
+        kmax = max(kmax, kk);
+        reinterpret_cast<uint32_t*>(&sm.keys[((size_t)f * NKQ + NR / 4) * kThreads + tid])[NR % 4] = kk;
+      }
+    __syncthreads();  // the keys are complete
     // ---- radix select of the K-th largest key.  The keys' top bits are mostly exponent, so a
     // plain first pass piles 24K keys into a few bins (serialised shared atomics).  Instead the
     // first pass histograms only keys within 16 binades of the largest key, at 1/16 binade
@@ -716,21 +800,36 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     }
     // ---- the window's bin was found: every key above it wins, the keys in it are candidates.
-    // One scan sorts them: a group of four keys below the bin (almost all of them) costs one
-    // compare, and each of the ~1% that reach it takes a slot with a shared atomic.  The
-    // candidates, usually a few dozen, are ranked among themselves.  More candidates than fit:
-    // the general passes below.
+    // Two scans sort them without atomics: the first counts each thread's keys above the bin
+    // and in it, one block scan of both counts (packed in one word; each total is below 2^16)
+    // gives every thread its slots, and the second writes them.  A group of four keys below
+    // the bin (almost all of them) costs one compare per scan.  The candidates, usually a few
+    // dozen, are ranked among themselves.  More candidates than fit: the general passes below.
     bool fast = false;
     if (n_pass == 3) {
-      if (tid == 0) {
-        sm.scal[kScNAbove] = 0;
-        sm.scal[kScNCand] = 0;
-      }
-      __syncthreads();
       uint64_t* ckey = reinterpret_cast<uint64_t*>(sm.whist);
       int* cid = reinterpret_cast<int*>(ckey + kCandCap);
       const uint32_t lo_key = prefix, hi_key = prefix + (1u << 19);  // the bin is [lo_key, hi_key)
+      uint32_t n_up = 0, n_in = 0;
       if (owner)
+        for (int f = 0; f < 6; ++f)
+#pragma unroll
+          for (int q = 0; q < NKQ; ++q) {
+            const uint4 v = sm.keys[((size_t)f * NKQ + q) * kThreads + tid];
+            if (max(max(v.x, v.y), max(v.z, v.w)) < lo_key) continue;
+            const uint32_t kk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const bool live = 4 * q + i < NK;
+              n_up += live && kk[i] >= hi_key;
+              n_in += live && kk[i] >= lo_key && kk[i] < hi_key;
+            }
+          }
+      uint32_t all;
+      const uint32_t packed = n_up | (n_in << 16);
+      const uint32_t excl = block_inclusive_sum(packed, sm.warp_tot, &all) - packed;  // barriers inside
+      uint32_t slot_up = excl & 0xFFFFu, slot_in = excl >> 16;
+      if (owner && packed)
         for (int f = 0; f < 6; ++f)
 #pragma unroll
           for (int q = 0; q < NKQ; ++q) {
@@ -745,18 +844,22 @@ __global__ void __launch_bounds__(kThreads, 2)
               const uint64_t ck = ((uint64_t)kk[i] << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)g);
               const int id = (f * NK + u) * kThreads + tid;
               if (kk[i] >= hi_key) {
-                const int slot = atomicAdd(&sm.scal[kScNAbove], 1);
-                sm.gkey[slot] = ck;
-                sm.gid[slot] = id;
+                sm.gkey[slot_up] = ck;
+                sm.gid[slot_up] = id;
+                ++slot_up;
               } else {
-                const int c = atomicAdd(&sm.scal[kScNCand], 1);
-                if (c < kCandCap) {
-                  ckey[c] = ck;
-                  cid[c] = id;
+                if (slot_in < (uint32_t)kCandCap) {
+                  ckey[slot_in] = ck;
+                  cid[slot_in] = id;
                 }
+                ++slot_in;
               }
             }
           }
+      if (tid == 0) {
+        sm.scal[kScNAbove] = (int)(all & 0xFFFFu);
+        sm.scal[kScNCand] = (int)(all >> 16);
+      }
       __syncthreads();
       const int n_cand = sm.scal[kScNCand];
       if (n_cand <= kCandCap) {
