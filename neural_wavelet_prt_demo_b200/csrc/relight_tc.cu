@@ -94,6 +94,10 @@ struct TcParams {
   uint32_t* amax;   // calibration: per-layer activation maxima (float bits)
   uint32_t* err;
   int* tile_ctr;    // the next 128-pixel tile to take (zeroed before the launch)
+  // Shared-memory descriptors of every layer's B tile, its aux block and the output layer's
+  // FP16 tile, formed on the host with the weight region at address 0: the kernel adds the
+  // region's address (>> 4, no carry out of the 14-bit field below 256 KB) in one step.
+  uint64_t bdesc[kMaxTcLayers], auxdesc[kMaxTcLayers], outdesc;
   // V_last, the FP32 3 x 64 output layer.  From the parameter space every output-dot FMA
   // takes its weight pair as an operand, without a shared-memory load.
   float vlast[3][64];
@@ -160,7 +164,7 @@ __device__ __forceinline__ bool wg_barrier_and(int g, bool pred) {
   return out != 0;
 }
 
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+__host__ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
 }
@@ -573,12 +577,16 @@ __device__ __forceinline__ void issue_layer(const TcLayer& L, bool with_aux, uin
   mma_commit(bar);
 }
 
-// The output layer T = V_last ReLU(h) on the tensor core: A = the last hidden layer's ReLU'd
-// activations as FP16 pairs in TMEM, B = V_last in FP16 (N = 16, channel c in row c), K = 64.
-__device__ __forceinline__ void issue_out(uint32_t wbase, uint32_t b_off, uint32_t sbo, uint32_t a_tmem,
-                                          uint32_t d_tmem, uint64_t* bar) {
+// Layer L of a fixed layer sequence: every layer is 64 wide, the step count and the aux flag
+// are compile-time, and the descriptors come precomputed (b0, bd: the weight region's
+// address already added; ad: the warpgroup's aux block).  Nothing between the warpgroup
+// barrier and the first MMA but the fence and the descriptor add.
+template <int MODE, int S, bool AUX>
+__device__ __forceinline__ void issue_fixed(uint64_t b0, uint64_t ad, uint64_t bd, uint32_t a_tmem, uint32_t d_tmem,
+                                            uint64_t* bar) {
   tc_fence_after();
-  issue_steps<kTcBf16, 4>(d_tmem, a_tmem, smem_desc(wbase + b_off, 128u, sbo), idesc_f16(16));
+  issue_steps<MODE, S>(d_tmem, a_tmem, b0, MODE == kTcFp8 ? idesc_e4m3(64) : idesc_bf16(64));
+  if (AUX) mma_ss(d_tmem, ad, bd, idesc_bf16(64), 1u);
   mma_commit(bar);
 }
 
@@ -635,6 +643,33 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   const uint32_t aux_base = smem_u32(aux + g * kAuxBytes);
   const uint32_t aux_row = aux_base + core_off(row, 0, 256u);
   uint64_t* acc_bar = &bars->acc_full[g];
+  // The warp that issues this warpgroup's MMAs.  Warp w runs on SM sub-partition w % 4, so
+  // taking warp g % 4 of warpgroup g spreads the five issuing warps over the four
+  // sub-partitions instead of stacking them on one.
+  const int lead = g & 3;
+  const uint64_t wb16 = (uint64_t)(wbase >> 4);
+  const uint64_t aux_desc = smem_desc(aux_base, 128u, 256u);
+  // fixed sequences: K steps of the first layer (hash features) and of the 64-wide ones
+  constexpr int kS0 = MODE == kTcFp8 ? 1 : DMAX / 16;
+  constexpr int kS1 = MODE == kTcFp8 ? 2 : 4;
+  auto issue_next = [&](int nl) {
+    if constexpr (SHAPE != kShapePlan) {
+      if (OUT_TC && nl == n_layers) {
+        tc_fence_after();
+        issue_steps<kTcBf16, 4>(d_tmem, d_tmem + 32u, p.outdesc + wb16, idesc_f16(16));
+        mma_commit(acc_bar);
+      } else if (nl == 0) {
+        issue_fixed<MODE, kS0, Sh::aux == 0>(p.bdesc[0] + wb16, aux_desc, p.auxdesc[0] + wb16, a_tmem, d_tmem,
+                                              acc_bar);
+      } else if (nl == Sh::aux) {
+        issue_fixed<MODE, kS1, true>(p.bdesc[nl] + wb16, aux_desc, p.auxdesc[nl] + wb16, a_tmem, d_tmem, acc_bar);
+      } else {
+        issue_fixed<MODE, kS1, false>(p.bdesc[nl] + wb16, aux_desc, 0ull, a_tmem, d_tmem, acc_bar);
+      }
+    } else {
+      issue_layer<MODE>(p.layers[nl], p.layers[nl].aux != 0, wbase, a_tmem, aux_base, d_tmem, acc_bar);
+    }
+  };
 
   uint32_t ph = 0;
   // Tiles come from the launch's counter, one atomic per tile and warpgroup, so that tiles of
@@ -676,9 +711,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     tc_fence_before();
     fence_proxy_async_smem();
     ok = wg_barrier_and(g, ok);
-    if (ok && q == 0 && elect_one())
-      issue_layer<MODE>(p.layers[0], SHAPE ? Sh::aux == 0 : p.layers[0].aux != 0, wbase, a_tmem, aux_base, d_tmem,
-                        acc_bar);
+    if (ok && q == lead && elect_one()) issue_next(0);
     // T_k -> clamped Kahan sums, then the next wavelet's first-layer operand
     auto finish_wavelet = [&](int k, float t0, float t1, float t2) {
       const float* Lk = J.strength + (size_t)k * 3;
@@ -795,13 +828,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
         if (!ok) break;
-        if (q == 0 && elect_one()) {
-          if (OUT_TC && nl == n_layers)
-            issue_out(wbase, p.out_b_off, p.out_sbo, d_tmem + 32u, d_tmem, acc_bar);
-          else
-            issue_layer<MODE>(p.layers[nl], SHAPE ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
-                              d_tmem, acc_bar);
-        }
+        if (q == lead && elect_one()) issue_next(nl);
         if (is_out) finish_wavelet(k, tk0, tk1, tk2);  // under the next wavelet's first MMA
         if (OUT_TC && nl == n_layers && k + 1 < K) {
           // the next wavelet's first-layer operand into the A columns, which the output MMA
@@ -824,7 +851,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     ok = wg_barrier_and(g, ok);
   }
   // every MMA this warpgroup issued has completed before TMEM is released
-  if (q == 0 && elect_one()) {  // the same lane that issued: a commit tracks its own thread's MMAs
+  if (q == lead && elect_one()) {  // the same lane that issued: a commit tracks its own thread's MMAs
     mma_commit(&bars->done[g]);
     wait_bounded(&bars->done[g], 0, p.err);
   }
@@ -1132,6 +1159,8 @@ int shape_of(const TcPlan& P, const NetDims& d) {
     for (int l = 0; l < nl; ++l) {
       const TcLayer& L = P.layers[l];
       if (L.n != 64 || !L.relu || (L.aux != 0) != (l == aux) || (L.fin != 0) != (l == nl - 1)) return false;
+      // the fixed kernels issue K = the hash features (padded to one FP8 step) first, then 64
+      if (l == 0 ? (L.k < enc || L.k > 32) : L.k != 64) return false;
     }
     return true;
   };
@@ -1216,6 +1245,11 @@ void launch_relight_tc(const NetDims& d, const HashLevels& hl, const float* hash
   p.wblob_bytes = P.blob_bytes;
   p.out_b_off = P.out_b_off;
   p.out_sbo = P.out_sbo;
+  for (int l = 0; l < P.n_layers; ++l) {
+    p.bdesc[l] = smem_desc(P.layers[l].b_off, 128u, P.layers[l].b_sbo);
+    p.auxdesc[l] = P.layers[l].aux ? smem_desc(P.layers[l].aux_off, 128u, 256u) : 0ull;
+  }
+  p.outdesc = P.out_sbo ? smem_desc(P.out_b_off, 128u, P.out_sbo) : 0ull;
   encode_weight_map(&p.wmap, blob_dev, P.blob_bytes, &p.w_boxes, &p.w_box_rows);
   std::memcpy(p.vlast, P.vlast, sizeof(p.vlast));
   std::memcpy(p.layers, P.layers, sizeof(P.layers));
