@@ -299,6 +299,16 @@ __device__ __forceinline__ uint32_t pack_e4m3x4(float x0, float x1, float x2, fl
 __device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 
+// Asynchronous global -> shared copies (cp.async): 16 bytes bypassing L1, or 4 bytes.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
                : "memory");
@@ -434,13 +444,28 @@ __device__ __forceinline__ void hash_encode_bf16(const HashLevels& hl, const flo
   }
 }
 
+// A tile's hash features in shared memory: one row of DMAX / 2 BF16 pairs per pixel, in
+// 16-byte chunks whose order within the row is XOR-swizzled by the row, so that a warp's
+// 16-byte loads of one chunk index (32 consecutive rows) are free of bank conflicts.
+template <int DMAX>
+struct EncRow {
+  static constexpr int kChunks = DMAX / 8;  // 16-byte chunks per row: 4 or 2
+  uint4* base;                              // this row
+  int swz;
+  __device__ __forceinline__ EncRow(uint32_t* tile_encs, int row)
+      : base(reinterpret_cast<uint4*>(tile_encs) + row * kChunks),
+        swz(kChunks == 4 ? (row >> 1) & 3 : (row >> 2) & 1) {}
+  __device__ __forceinline__ uint4 get(int c) const { return base[c ^ swz]; }
+  __device__ __forceinline__ void put(int c, uint4 v) const { base[c ^ swz] = v; }
+};
+
 // First-layer operand of wavelet k, hash(p) * E_k -> TMEM A columns.  BF16: one packed
 // bf16x2 multiply per feature pair of the BF16 hash features and the BF16 embedding row eh
 // (the exact product, rounded once).  Calibration: the same product from the FP32 row ek,
 // recording max |hash(p) * E_k| in amax[0].  FP8: from the FP32 row, scaled by cp_scale and
 // rounded to E4M3, zero-padded to K = 32.
 template <int DMAX, int MODE>
-__device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __restrict__ ek,
+__device__ __forceinline__ void store_cp(const EncRow<DMAX>& enc, const float* __restrict__ ek,
                                          const uint32_t* __restrict__ eh, uint32_t a_taddr, float cp_scale,
                                          uint32_t* amax) {
   constexpr int NW = MODE == kTcFp8 ? 8 : DMAX / 2;
@@ -449,11 +474,10 @@ __device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __r
 #pragma unroll
     for (int c = 0; c < DMAX / 8; ++c) {
       const uint4 e = __ldg(reinterpret_cast<const uint4*>(eh) + c);
-      const uint32_t ev[4] = {e.x, e.y, e.z, e.w};
+      const uint4 h = enc.get(c);
+      const uint32_t ev[4] = {e.x, e.y, e.z, e.w}, hv[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(cp[c * 4 + i]) : "r"(enc_s[(c * 4 + i) * kTile]), "r"(ev[i]));
-      }
+      for (int i = 0; i < 4; ++i) asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(cp[c * 4 + i]) : "r"(hv[i]), "r"(ev[i]));
     }
     if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
     else tmem_st8(a_taddr, cp);
@@ -464,8 +488,8 @@ __device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __r
   for (int c = 0; c < DMAX / 8; ++c) {
     const float4 e0 = __ldg(reinterpret_cast<const float4*>(ek + c * 8));
     const float4 e1 = __ldg(reinterpret_cast<const float4*>(ek + c * 8 + 4));
-    const uint32_t h0 = enc_s[(c * 4 + 0) * kTile], h1 = enc_s[(c * 4 + 1) * kTile];
-    const uint32_t h2 = enc_s[(c * 4 + 2) * kTile], h3 = enc_s[(c * 4 + 3) * kTile];
+    const uint4 h = enc.get(c);
+    const uint32_t h0 = h.x, h1 = h.y, h2 = h.z, h3 = h.w;
     const float x0 = __fmul_rn(bf16_lo(h0), e0.x), x1 = __fmul_rn(bf16_hi(h0), e0.y);
     const float x2 = __fmul_rn(bf16_lo(h1), e0.z), x3 = __fmul_rn(bf16_hi(h1), e0.w);
     const float x4 = __fmul_rn(bf16_lo(h2), e1.x), x5 = __fmul_rn(bf16_hi(h2), e1.y);
@@ -496,6 +520,21 @@ __device__ __forceinline__ void store_cp(const uint32_t* enc_s, const float* __r
   if constexpr (MODE == kTcCalibrate) record_amax(amax, __float_as_uint(m));
 }
 
+// store_cp's BF16 form with the embedding row taken from shared memory.
+template <int DMAX>
+__device__ __forceinline__ void store_cp_smem(const EncRow<DMAX>& enc, const uint4* e_row, uint32_t a_taddr) {
+  uint32_t cp[DMAX / 2];
+#pragma unroll
+  for (int c = 0; c < DMAX / 8; ++c) {
+    const uint4 e = e_row[c], h = enc.get(c);
+    const uint32_t ev[4] = {e.x, e.y, e.z, e.w}, hv[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(cp[c * 4 + i]) : "r"(hv[i]), "r"(ev[i]));
+  }
+  if constexpr (DMAX == 32) tmem_st16(a_taddr, cp);
+  else tmem_st8(a_taddr, cp);
+}
+
 __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long tile) {
   int lo = 0, hi = n_jobs - 1;
   while (lo < hi) {
@@ -506,7 +545,13 @@ __device__ __forceinline__ int find_job(const TcJob* jobs, int n_jobs, long long
   return lo;
 }
 
-struct __align__(8) TcBarriers {
+constexpr int kBatch = 8, kRing = 2 * kBatch;
+struct __align__(16) TcBarriers {
+  // Per warpgroup, rings of kRing slots: the BF16 embedding rows E_j (read for wavelet j's
+  // first-layer operand) and the strengths L_j (read after wavelet j's output layer), copied
+  // in by cp.async kBatch wavelets at a time (slot j % kRing).
+  uint4 e_ring[kNWG][kRing][4];
+  float4 l_ring[kNWG][kRing];
   uint64_t acc_full[kNWG];  // MMA commit -> epilogue of that warpgroup's tile
   uint64_t done[kNWG];      // final commit before TMEM is released
   uint64_t wload;           // the weight blob's TMA load
@@ -601,7 +646,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;                                                  // weight blob
   uint8_t* aux = smem + weight_region_bytes(p.w_boxes, p.w_box_rows);  // [kNWG][kAuxBytes]
-  uint32_t* encs = reinterpret_cast<uint32_t*>(aux + kNWG * kAuxBytes);  // [kNWG][DMAX/2][kTile]
+  uint32_t* encs = reinterpret_cast<uint32_t*>(aux + kNWG * kAuxBytes);  // [kNWG][kTile][DMAX/2], swizzled
   TcBarriers* bars = reinterpret_cast<TcBarriers*>(encs + kNWG * (DMAX / 2) * kTile);
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -647,6 +692,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
   // taking warp g % 4 of warpgroup g spreads the five issuing warps over the four
   // sub-partitions instead of stacking them on one.
   const int lead = g & 3;
+  const int fetcher = (g + 1) & 3;  // the warp that fills the warpgroup's rings (never the issuer)
   const uint64_t wb16 = (uint64_t)(wbase >> 4);
   const uint64_t aux_desc = smem_desc(aux_base, 128u, 256u);
   // fixed sequences: K steps of the first layer (hash features) and of the 64-wide ones
@@ -667,7 +713,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         issue_fixed<MODE, kS1, false>(p.bdesc[nl] + wb16, aux_desc, 0ull, a_tmem, d_tmem, acc_bar);
       }
     } else {
-      issue_layer<MODE>(p.layers[nl], p.layers[nl].aux != 0, wbase, a_tmem, aux_base, d_tmem, acc_bar);
+      issue_layer<MODE>(p.layers[nl], Sh::aux >= 0 ? Sh::aux == nl : p.layers[nl].aux != 0, wbase, a_tmem, aux_base,
+                        d_tmem, acc_bar);
     }
   };
 
@@ -685,14 +732,15 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     const int K = J.K;
     const long long px = J.px_begin + (t - J.tile_begin) * kTile + row;
     const bool valid = px < J.n_px;
-    uint32_t* enc_s = encs + g * (DMAX / 2) * kTile + row;  // this pixel's features, stride kTile
+    const EncRow<DMAX> enc_s(encs + g * (DMAX / 2) * kTile, row);  // this pixel's features
     if (valid) {
       uint32_t enc[DMAX / 2];
       const float4* pr = reinterpret_cast<const float4*>(J.packed) + px * 4;
       const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3);
       hash_encode_bf16<DMAX>(p.hl, p.hash, r0.x, r0.y, r0.z, enc);
 #pragma unroll
-      for (int i = 0; i < DMAX / 2; ++i) enc_s[i * kTile] = enc[i];
+      for (int c = 0; c < DMAX / 8; ++c)
+        enc_s.put(c, make_uint4(enc[4 * c], enc[4 * c + 1], enc[4 * c + 2], enc[4 * c + 3]));
       // aux operand: the 13 remapped G-buffer values followed by ones
       st_shared_v4(aux_row, pack_bf16(r0.w, r1.x), pack_bf16(r1.y, r1.z), pack_bf16(r1.w, r2.x),
                    pack_bf16(r2.y, r2.z));
@@ -700,7 +748,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
                    pack_bf16(1.f, 1.f));
     } else {
 #pragma unroll
-      for (int i = 0; i < DMAX / 2; ++i) enc_s[i * kTile] = 0u;
+      for (int c = 0; c < DMAX / 8; ++c) enc_s.put(c, make_uint4(0u, 0u, 0u, 0u));
       st_shared_v4(aux_row, 0, 0, 0, 0);
       st_shared_v4(aux_row + 128u, 0, 0, 0, 0);
     }
@@ -714,10 +762,17 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     if (ok && q == lead && elect_one()) issue_next(0);
     // T_k -> clamped Kahan sums, then the next wavelet's first-layer operand
     auto finish_wavelet = [&](int k, float t0, float t1, float t2) {
-      const float* Lk = J.strength + (size_t)k * 3;
-      float u0 = __fmul_rn(__ldg(Lk + 0), t0);
-      float u1 = __fmul_rn(__ldg(Lk + 1), t1);
-      float u2 = __fmul_rn(__ldg(Lk + 2), t2);
+      float L0, L1, L2;
+      if constexpr (OUT_TC) {
+        const float4 Lk = bars->l_ring[g][k % kRing];
+        L0 = Lk.x; L1 = Lk.y; L2 = Lk.z;
+      } else {
+        const float* Lk = J.strength + (size_t)k * 3;
+        L0 = __ldg(Lk + 0); L1 = __ldg(Lk + 1); L2 = __ldg(Lk + 2);
+      }
+      float u0 = __fmul_rn(L0, t0);
+      float u1 = __fmul_rn(L1, t1);
+      float u2 = __fmul_rn(L2, t2);
       if (p.clamp) { u0 = fmaxf(u0, 0.f); u1 = fmaxf(u1, 0.f); u2 = fmaxf(u2, 0.f); }
       if (p.kahan) {
         float y, z;
@@ -825,16 +880,29 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
           break;
         }
         const int nl = (l + 1 == n_steps) ? 0 : l + 1;
+        if (pre_out && q == fetcher) cp_async_wait_all();  // the rings, before this barrier
         tc_fence_before();
         ok = wg_barrier_and(g, ok);
         if (!ok) break;
         if (q == lead && elect_one()) issue_next(nl);
+        if (OUT_TC && l == 0 && q == fetcher && k % kBatch == 0) {
+          // E_k+1..k+8 and L_k..k+7 into the rings, by a warp that would otherwise only wait
+          // for this layer's MMAs; waited for before this wavelet's last hidden-layer barrier
+          constexpr int C = DMAX / 8;
+          const int j = lane / C;
+          if (j < kBatch && k + 1 + j < K)
+            cp_async16(smem_u32(&bars->e_ring[g][(k + 1 + j) % kRing][lane % C]),
+                       J.emb_h + (size_t)(k + 1 + j) * (p.enc_dims / 2) + (lane % C) * 4);
+          if (lane < 3 * kBatch && k + lane / 3 < K)
+            cp_async4(smem_u32(reinterpret_cast<float*>(&bars->l_ring[g][(k + lane / 3) % kRing]) + lane % 3),
+                      J.strength + (size_t)k * 3 + lane);
+          cp_async_commit();
+        }
         if (is_out) finish_wavelet(k, tk0, tk1, tk2);  // under the next wavelet's first MMA
         if (OUT_TC && nl == n_layers && k + 1 < K) {
           // the next wavelet's first-layer operand into the A columns, which the output MMA
           // (operand in [64, 96), accumulator in [32, 48)) does not touch
-          store_cp<DMAX, MODE>(enc_s, J.emb_k + (size_t)(k + 1) * p.enc_dims,
-                               J.emb_h + (size_t)(k + 1) * (p.enc_dims / 2), a_taddr, p.cp_scale, p.amax);
+          store_cp_smem<DMAX>(enc_s, bars->e_ring[g][(k + 1) % kRing], a_taddr);
           tmem_wait_st();
         }
       }
@@ -850,6 +918,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
     if (q == 0 && lane == 0) bars->tile_slot[g] = atomicAdd(p.tile_ctr, 1);
     ok = wg_barrier_and(g, ok);
   }
+  if (OUT_TC && q == fetcher) cp_async_wait_all();  // no ring copy outlives the CTA (a timed-out exit)
   // every MMA this warpgroup issued has completed before TMEM is released
   if (q == lead && elect_one()) {  // the same lane that issued: a commit tracks its own thread's MMAs
     mma_commit(&bars->done[g]);
