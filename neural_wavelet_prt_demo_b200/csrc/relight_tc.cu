@@ -32,12 +32,15 @@
 // Thread (warp w, lane l) owns tile row 32*(w%4)+l, the TMEM lane it may access.  Per
 // layer: wait on the tile's commit barrier -> tcgen05.ld -> ReLU + cvt.rn.relu.bf16x2 ->
 // tcgen05.st into the A columns -> warpgroup barrier (bar.red.and carrying the "no
-// timeout" vote) -> an elected lane of warp 0 issues the next layer's MMAs and commits
-// them.  In the BF16 fixed-sequence kernels the last hidden layer's FP16 operand goes to
+// timeout" vote) -> an elected lane of warp g % 4 of warpgroup g issues the next layer's MMAs
+// and commits them (so the five issuing warps spread over the SM's four sub-partitions).  In the BF16 fixed-sequence kernels the last hidden layer's FP16 operand goes to
 // accumulator columns [64, 96), the next wavelet's first-layer operand hash(p) * E_k+1 is
 // written into the A columns while the output MMA runs, and T_k's clamped Kahan sum is formed
 // after the hand-off to that next wavelet; the FP32-dot forms do all three in the last hidden
-// layer's epilogue.  Warpgroups take tiles from a per-launch counter, so tiles of different
+// layer's epilogue.  In the BF16 fixed-sequence kernels the embedding rows and strengths those
+// two steps read come from per-warpgroup shared-memory rings that a non-issuing warp fills by
+// cp.async, eight wavelets ahead of use: read from L2 they put two L2 latencies on every
+// wavelet's chain.  Warpgroups take tiles from a per-launch counter, so tiles of different
 // cost (requests of different K) balance across the SMs.  The two standard networks run
 // kernels specialised on their layer sequence (ShapeOf), every other supported network a
 // generic form that reads the sequence from the plan.  Every wait is bounded by
