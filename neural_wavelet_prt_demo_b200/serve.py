@@ -273,6 +273,16 @@ class RelightServer:
         self.face_size, self.enc_dims = info.face_size, info.enc_dims
         self.quanta = 0
         self.max_active = 0
+        # pinned staging buffers for new env maps, reused round robin (a pinned allocation per
+        # request costs milliseconds of host time, which the launch loop cannot spare); each
+        # buffer's event marks its last upload as done before the buffer is overwritten
+        # output buffers of retired requests, per resolution, handed to the next admitted
+        # request of that resolution (with hundreds of requests admitted, fresh frame-sized
+        # allocations fall through the caching allocator to cudaMalloc)
+        self._out_pool: Dict[int, List] = {}
+        self._staging: List = []
+        self._staging_ev: List = []
+        self._staging_next = 0
 
     def _prepare(self, r: Request) -> None:
         """Output buffers and the env wavelet table, stream-ordered before its first quantum."""
@@ -280,15 +290,20 @@ class RelightServer:
         fr = self.frames[r.res]
         # outputs are indexed by absolute pixel: a band's buffer covers the whole frame, which
         # also lets a split request's owner receive the other ranks' bands into it
-        ind = torch.empty((fr.width * fr.height, 4), dtype=torch.float32, device=fr.fbPredictedIndirect.device)
-        wd = torch.empty_like(ind)
+        pool = self._out_pool.setdefault(r.res, [])
+        if pool:
+            ind, wd = pool.pop()
+        else:
+            ind = torch.empty((fr.width * fr.height, 4), dtype=torch.float32, device=fr.fbPredictedIndirect.device)
+            wd = torch.empty_like(ind)
         if r.env_kind == "new":
             host = torch.from_numpy(np.ascontiguousarray(r.faces, np.float32))
             if self.on_gpu:
                 # through pinned memory: a copy from pageable memory may wait for the stream,
                 # i.e. for the launches already queued
-                host = torch.empty(host.shape, dtype=torch.float32, pin_memory=True).copy_(host)
-            faces = host.to(ind.device, non_blocking=True)
+                faces = self._upload_pinned(host, ind.device)
+            else:
+                faces = host.to(ind.device)
         elif r.env_kind == "rot":
             from .engine import env_rotate
             faces = env_rotate(self.base_faces[r.base_env], r.R)
@@ -296,6 +311,30 @@ class RelightServer:
             raise ValueError(f"unknown env kind {r.env_kind!r}")
         r.env_id = self.e.addEnvironmentFaces(faces, r.K)
         r.outputs = (ind, wd, faces)
+
+    STAGING_BUFFERS = 32
+    ADMIT_SLICE_S = 0.002  # host time spent admitting before a free launch slot is filled
+
+    def _upload_pinned(self, host, device):
+        """Copies host faces to a new device tensor through the reused pinned staging pool."""
+        torch = self.torch
+        i = self._staging_next
+        self._staging_next = (i + 1) % self.STAGING_BUFFERS
+        if i >= len(self._staging):
+            self._staging.append(torch.empty(host.shape, dtype=torch.float32, pin_memory=True))
+            self._staging_ev.append(None)
+        buf = self._staging[i]
+        if buf.shape != host.shape:
+            buf = self._staging[i] = torch.empty(host.shape, dtype=torch.float32, pin_memory=True)
+            self._staging_ev[i] = None
+        if self._staging_ev[i] is not None:
+            self._staging_ev[i].synchronize()  # the upload 32 requests ago: long complete
+        buf.copy_(host)
+        faces = buf.to(device, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self._staging_ev[i] = ev
+        return faces
 
     def _end_failed(self, r: Request, t: float) -> None:
         """Ends a request that failed after admission: returns its budget and env table."""
@@ -335,6 +374,9 @@ class RelightServer:
         self.e.releaseEnvironmentMap(r.env_id)
         r.env_id = -1
         if not self.keep_outputs:
+            # the request's last launch has completed (its event was waited for)
+            if r.outputs:
+                self._out_pool.setdefault(r.res, []).append((r.outputs[0], r.outputs[1]))
             r.outputs = ()
 
     def _refuse(self, r: Request, status: str, t: float) -> None:
@@ -381,6 +423,11 @@ class RelightServer:
             # admission (FCFS under the byte budget; over-budget and stale requests are refused)
             t_ph = time.perf_counter()
             while queue and (self.max_active_cap is None or len(active) < self.max_active_cap):
+                # a launch slot is free and work is admitted: launch before admitting more, so a
+                # burst of arrivals does not leave the GPU without queued work
+                if (active and len(in_flight) < self.max_in_flight
+                        and time.perf_counter() - t_ph > self.ADMIT_SLICE_S):
+                    break
                 r = queue[0]
                 try:
                     validate_request(r, len(self.frames), self.face_size, len(self.base_faces))
