@@ -791,7 +791,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
         tmem_wait_st();
       }
     };
-    float tk0 = 0.f, tk1 = 0.f, tk2 = 0.f;  // OUT_TC: T_k, summed after the next hand-off
+    float tk0 = 0.f, tk1 = 0.f, tk2 = 0.f;  // OUT_TC: T_k, summed during the next wavelet
     for (int k = 0; k < K && ok; ++k) {
 #pragma unroll(SHAPE ? Sh::nl + (OUT_TC ? 1 : 0) : 1)
       for (int l = 0; l < n_steps; ++l) {
@@ -901,7 +901,9 @@ __global__ void __launch_bounds__(kThreads, 1) relight_tc_kernel(const __grid_co
                       J.strength + (size_t)k * 3 + lane);
           cp_async_commit();
         }
-        if (is_out) finish_wavelet(k, tk0, tk1, tk2);  // under the next wavelet's first MMA
+        // T_k's clamped Kahan update waits one more step: under the next wavelet's second layer,
+        // whose MMAs take longer than its first layer's, so that it stays off the chain
+        if (OUT_TC && l == 1 && k > 0) finish_wavelet(k - 1, tk0, tk1, tk2);
         if (OUT_TC && nl == n_layers && k + 1 < K) {
           // the next wavelet's first-layer operand into the A columns, which the output MMA
           // (operand in [64, 96), accumulator in [32, 48)) does not touch
