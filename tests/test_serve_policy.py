@@ -138,3 +138,62 @@ def test_class_latency_splits_at_720p():
     c = serve.class_latency(reqs, frames)
     assert c["small"]["done"] == 2 and c["large"]["done"] == 2
     assert c["small"]["p50_ms"] == pytest.approx(7.0) and c["large"]["p50_ms"] == pytest.approx(40.0)
+
+
+class _PoolFrame:
+    def __init__(self, w, h):
+        import torch
+        self.width, self.height = w, h
+        self.fbPredictedIndirect = torch.zeros((w * h, 4))
+
+
+class _PoolEngine:
+    """Stand-in relight that checks no two live requests ever write the same output buffer."""
+
+    class _Info:
+        face_size, enc_dims = 4, 16
+
+    def __init__(self):
+        self.live = {}      # env id -> id of the output buffer its request writes
+        self.next = 0
+        self.violations = 0
+
+    def networkInfo(self):
+        return self._Info()
+
+    def addEnvironmentFaces(self, faces, K):
+        self.next += 1
+        return self.next - 1
+
+    def releaseEnvironmentMap(self, env):
+        self.live.pop(env, None)
+
+    def relightRanges(self, ranges, cfg=None):
+        for env, frame, ind, wd, b, e in ranges:
+            owner = self.live.setdefault(env, id(ind))
+            if owner != id(ind) or any(o == id(ind) for k, o in self.live.items() if k != env):
+                self.violations += 1
+            ind[b:e] = float(env)
+            wd[b:e] = float(env) + 1.0
+
+    def TCNNSync(self):
+        pass
+
+
+def test_output_buffers_are_reused_and_never_shared_by_live_requests():
+    """Retired requests hand their output buffers to later requests of the same resolution
+    (no fresh frame-sized allocation per request), and no two live requests share one.  A
+    request holds its buffers from admission until its last launch has completed: with at most
+    two admitted and two launches in flight, at most six pairs per resolution are ever made."""
+    frames_wh = [(16, 8), (32, 16), (48, 24)]
+    frames = [_PoolFrame(w, h) for w, h in frames_wh]
+    reqs = serve.make_stream(60, rate=1e5, seed=5, face_size=4, p_new=1.0, resolutions=frames_wh, ks=[4, 8])
+    eng = _PoolEngine()
+    srv = serve.RelightServer(eng, frames, [], precision="fp32", quantum_ms=1.0, est_evals_per_s=2e5, max_active=2)
+    out = srv.run(reqs, realtime=False)
+    assert out["done"] == len(reqs)
+    assert eng.violations == 0
+    for res in range(len(frames_wh)):
+        pool = srv._out_pool.get(res, [])
+        n_res = sum(1 for r in reqs if r.res == res)
+        assert 1 <= len(pool) <= 6 and 2 * len(pool) < n_res, (res, len(pool), n_res)
